@@ -1,0 +1,143 @@
+"""ctypes bindings for the two native libraries (C ABI in include/natinterp3d_b200.h).
+
+The libraries are loaded from ``natinterp3d_b200/lib``.  A missing CUDA
+library is an error, never a silent fallback: there is no CPU query path in
+this package.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+from . import _build
+
+c_int = ctypes.c_int
+c_int32 = ctypes.c_int32
+c_int64 = ctypes.c_int64
+c_void_p = ctypes.c_void_p
+c_double_p = ctypes.POINTER(ctypes.c_double)
+c_int32_p = ctypes.POINTER(ctypes.c_int32)
+c_size_t = ctypes.c_size_t
+
+# status codes shared by both libraries (include/natinterp3d_b200.h)
+NIF_OK = 0
+NIF_ERR_ARG = -1
+NIF_ERR_DEGENERATE = -2
+NIF_ERR_NOMEM = -3
+NIF_ERR_INTERNAL = -4
+NIF_ERR_OVERFLOW = -5
+NIF_ERR_WALK = -6
+NIF_ERR_CUDA = -7
+NIF_ERR_CAPACITY = -8
+NIF_ERR_WORKSPACE = -9
+
+_ERR_NAMES = {
+    NIF_ERR_ARG: 'invalid argument',
+    NIF_ERR_DEGENERATE: 'degenerate key set',
+    NIF_ERR_NOMEM: 'out of memory',
+    NIF_ERR_INTERNAL: 'internal error',
+    NIF_ERR_OVERFLOW: 'nnz overflow',
+    NIF_ERR_WALK: 'point-location walk step limit reached',
+    NIF_ERR_CUDA: 'CUDA error',
+    NIF_ERR_CAPACITY: 'per-query capacity exceeded',
+    NIF_ERR_WORKSPACE: 'workspace too small',
+}
+
+
+class NativeError(RuntimeError):
+    def __init__(self, code, what):
+        self.code = code
+        super().__init__('%s failed: %s (status %d)' % (what, _ERR_NAMES.get(code, 'error'), code))
+
+
+def check(code, what):
+    if code != NIF_OK:
+        raise NativeError(code, what)
+
+
+def _ptr(a, ctype):
+    return a.ctypes.data_as(ctypes.POINTER(ctype))
+
+
+# --------------------------------------------------------------------------
+# host mesh constructor
+# --------------------------------------------------------------------------
+_mesh_lib = None
+
+
+def mesh_lib():
+    global _mesh_lib
+    if _mesh_lib is None:
+        path = _build.MESH_SO
+        if not os.path.exists(path):
+            path = _build.build_mesh_lib()
+        lib = ctypes.CDLL(path)
+        lib.nif_mesh_build.argtypes = [c_double_p, c_int, ctypes.POINTER(c_void_p)]
+        lib.nif_mesh_build.restype = c_int
+        lib.nif_mesh_free.argtypes = [c_void_p]
+        lib.nif_mesh_free.restype = None
+        lib.nif_mesh_sizes.argtypes = [c_void_p, ctypes.POINTER(c_int), ctypes.POINTER(c_int)]
+        lib.nif_mesh_sizes.restype = c_int
+        lib.nif_mesh_export.argtypes = [c_void_p, c_double_p, c_int32_p, c_int32_p]
+        lib.nif_mesh_export.restype = c_int
+        lib.nif_mesh_degeneracies.argtypes = [c_void_p, ctypes.POINTER(c_int),
+                                              ctypes.POINTER(c_int)]
+        lib.nif_mesh_degeneracies.restype = c_int
+        lib.nif_mesh_native.argtypes = [c_void_p]
+        lib.nif_mesh_native.restype = c_void_p
+        _mesh_lib = lib
+    return _mesh_lib
+
+
+class HostMesh:
+    """natinterp3d's Delaunay mesh of a (centred) key set, built on the host.
+
+    Owns the natinterp3d mesh object; ``export()`` returns the packed arrays
+    (vxyz [N+4, 3] float64, tet_v [T, 4] int32, tet_n [T, 4] int32).
+    """
+
+    def __init__(self, keys_centered):
+        keys = np.ascontiguousarray(keys_centered, dtype=np.float64)
+        if keys.ndim != 2 or keys.shape[1] != 3:
+            raise ValueError('Data points must have shape (num_data_points, 3)')
+        self._lib = mesh_lib()
+        self._h = c_void_p()
+        self.n = int(keys.shape[0])
+        rc = self._lib.nif_mesh_build(_ptr(keys, ctypes.c_double), self.n, ctypes.byref(self._h))
+        if rc == NIF_ERR_DEGENERATE or rc == NIF_ERR_ARG:
+            raise ValueError('natinterp3d cannot triangulate this key set: it needs at least one '
+                             'point and a non-zero, finite extent along every axis')
+        check(rc, 'nif_mesh_build')
+        nv, nt = c_int(), c_int()
+        check(self._lib.nif_mesh_sizes(self._h, ctypes.byref(nv), ctypes.byref(nt)),
+              'nif_mesh_sizes')
+        self.n_vertices, self.n_tets = nv.value, nt.value
+
+    def export(self):
+        vxyz = np.empty((self.n_vertices, 3), np.float64)
+        tet_v = np.empty((self.n_tets, 4), np.int32)
+        tet_n = np.empty((self.n_tets, 4), np.int32)
+        check(self._lib.nif_mesh_export(self._h, _ptr(vxyz, ctypes.c_double),
+                                         _ptr(tet_v, ctypes.c_int32), _ptr(tet_n, ctypes.c_int32)),
+              'nif_mesh_export')
+        return vxyz, tet_v, tet_n
+
+    def degeneracies(self):
+        a, b = c_int(), c_int()
+        check(self._lib.nif_mesh_degeneracies(self._h, ctypes.byref(a), ctypes.byref(b)),
+              'nif_mesh_degeneracies')
+        return {'coplanar': a.value, 'cospherical': b.value}
+
+    def native_pointer(self):
+        return self._lib.nif_mesh_native(self._h)
+
+    def close(self):
+        if getattr(self, '_h', None) is not None and self._h.value:
+            self._lib.nif_mesh_free(self._h)
+            self._h = c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
