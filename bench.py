@@ -1,0 +1,372 @@
+"""Benchmark of the Sibson query path on B200.
+
+Default workload (one step = one pass of the hot path over one batch):
+plain interpolate at scale -- 1,000,000 keys uniform in [0,1]^3 (float64),
+10,000,000 queries uniform in [0.02,0.98]^3 (float64), values D=3 float32
+N(0,1), seed 1.  The Delaunay construction (natinterp3d's own, on the host)
+is done once before timing, on both arms, as in natinterp3d's Interpolator.
+
+Our arm prints one JSON line with
+  value   queries/s with inputs resident in HBM (CUDA events, max over ranks)
+  e2e     queries/s through Interpolator.interpolate with host numpy buffers
+          (host->device copy of the queries and values, device->host copy of
+          the result inside the timed region)
+  roofline, cpu_baseline, clocks, gpu_launches.
+``--impl reference`` times natinterp3d's own CPU implementation (its C
+sources compiled in oracle/_ref; mesh built by its own constructor) with all
+host threads on a bounded sample of the same workload.
+
+Multi-GPU (torchrun): every rank builds the same mesh and processes its own
+batch of queries (weak scaling, no data-path collective).
+"""
+import argparse
+import ctypes
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = 'Sibson queries/s at 1M keys (plain, fwd+bwd, batched) vs CPU OpenMP, 1 B200'
+WORKLOAD = ('plain interpolate at scale: {keys:,} keys U[0,1]^3 float64, {queries:,} queries '
+            'U[0.02,0.98]^3 float64, values D={dim} float32 N(0,1), seed {seed}')
+
+# FP64 operations per unit of work, counted as natinterp3d's C evaluates them
+# (each add, subtract, multiply and divide is one flop; no fused multiply-add)
+FLOPS = {'orient': 23, 'insphere': 77, 'tet_cc': 79, 'tri_cc': 56, 'subcell': 89}
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument('--gpus', type=int, default=1)
+    p.add_argument('--steps', type=int, default=5)
+    p.add_argument('--warmup', type=int, default=3)
+    p.add_argument('--impl', default='ours', choices=['ours', 'reference'])
+    p.add_argument('--keys', type=int, default=1_000_000)
+    p.add_argument('--queries', type=int, default=10_000_000)
+    p.add_argument('--dim', type=int, default=3)
+    p.add_argument('--seed', type=int, default=1)
+    p.add_argument('--e2e-steps', type=int, default=3)
+    p.add_argument('--no-cpu-baseline', action='store_true')
+    return p.parse_args()
+
+
+def make_data(args, rank=0):
+    rng = np.random.default_rng(args.seed)
+    keys = rng.uniform(0.0, 1.0, (args.keys, 3))
+    values = rng.standard_normal((args.keys, args.dim)).astype(np.float32)
+    qrng = np.random.default_rng([args.seed, rank])
+    queries = qrng.uniform(0.02, 0.98, (args.queries, 3))
+    return keys, queries, values
+
+
+def host_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during a region."""
+    FIELDS = ('index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,'
+              'clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,'
+              'clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap')
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ['nvidia-smi', '-i', str(self.gpu), '--query-gpu=' + self.FIELDS,
+                 '--format=csv,noheader,nounits', '-lms', '200'],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, smax, reasons = [], None, set()
+        names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap']
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(',')]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == 'active':
+                    reasons.add(n)
+        if not sm:
+            return {'sm_mhz': None, 'sm_max_mhz': None, 'reasons': ['no samples'], 'samples': 0}
+        return {'sm_mhz': float(np.median(sm)), 'sm_max_mhz': smax, 'reasons': sorted(reasons),
+                'samples': len(sm)}
+
+
+# ---------------------------------------------------------------------------
+def flops_per_query(stats, gpu_walk_steps, n):
+    """Algorithmic FP64 flops per query of the GPU row kernel.
+
+    The kernel reads tet and face circumcentres from the per-mesh cache, so
+    per query it evaluates: 4 orientation tests per walk step, the insphere
+    tests, one virtual-tet circumcentre per boundary face, two fresh triangle
+    circumcentres and one subcell volume per new term, one subcell volume per
+    old term, one addition per term, and the normalisation."""
+    q = stats['queries']
+    terms = stats['old_terms'] + stats['new_terms']
+    total = (4 * FLOPS['orient'] * gpu_walk_steps / n * q
+             + FLOPS['insphere'] * stats['insphere']
+             + FLOPS['tet_cc'] * stats['boundary']
+             + 2 * FLOPS['tri_cc'] * stats['new_terms']
+             + FLOPS['subcell'] * terms
+             + terms + 3 * stats['neighbours'] + 4 * q)
+    return total / q
+
+
+def run_reference(args, rank, world):
+    """natinterp3d's own CPU implementation (oracle/_ref) on the host cores."""
+    if rank != 0:
+        return None
+    from oracle import oracle
+    if not oracle.ref_available():
+        print(json.dumps({'impl': 'reference', 'unavailable': 'natinterp3d reference library '
+                          'not built (oracle/_ref missing)'}))
+        return None
+    keys, queries, values = make_data(args)
+    nthreads = host_threads()
+    t0 = time.perf_counter()
+    ref = oracle.RefInterpolator(keys, num_threads=nthreads)
+    build_s = time.perf_counter() - t0
+    # bounded sample per step: about 2 s of wall time on this host
+    probe = queries[:50_000]
+    t0 = time.perf_counter()
+    ref.interpolate(probe, values)
+    rate = probe.shape[0] / (time.perf_counter() - t0)
+    sample = int(min(queries.shape[0], max(50_000, rate * 2.0)))
+    qs = queries[:sample]
+    for _ in range(max(1, args.warmup)):
+        ref.interpolate(qs[:min(sample, 100_000)], values)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        ref.interpolate(qs, values)
+        times.append(time.perf_counter() - t0)
+    sec = float(np.median(times))
+    value = sample / sec
+    line = {
+        'impl': 'reference', 'metric': METRIC, 'value': value, 'unit': 'queries/s',
+        'n_gpus': world, 'steps': args.steps, 'warmup': args.warmup,
+        'ms_per_step': sec * 1e3, 'higher_is_better': True, 'scaling': 'weak',
+        'vs_baseline': None, 'dtype': 'f64', 'data': 'synthetic',
+        'config': {'workload': WORKLOAD.format(keys=args.keys, queries=args.queries, dim=args.dim,
+                                               seed=args.seed),
+                   'keys': args.keys, 'queries': args.queries, 'D': args.dim},
+        'cpu_baseline': {'value': value, 'unit': 'queries/s', 'cores': nthreads,
+                         'kind': 'reference',
+                         'sample': '%d of the %d queries per step (get_weights with %d OpenMP '
+                                   'threads + scipy W @ values), mesh built by natinterp3d in %.1f s'
+                                   % (sample, args.queries, nthreads, build_s)},
+        'e2e': {'value': value, 'unit': 'queries/s', 'h2d_bytes_per_step': 0,
+                'd2h_bytes_per_step': 0},
+    }
+    print(json.dumps(line))
+    return line
+
+
+def cpu_baseline(interp, queries, values):
+    """natinterp3d's own query code on the same mesh object, all host threads."""
+    from oracle import oracle
+    if not oracle.ref_available() or interp.host_mesh is None:
+        return None
+    nthreads = host_threads()
+    ptr = interp.host_mesh.native_pointer()
+    c = interp.centroid
+
+    def run(qs):
+        W = oracle.ref_query(ptr, np.ascontiguousarray(qs, np.float64) - c, interp.n_keys, nthreads)
+        return W @ values
+
+    probe = queries[:50_000]
+    run(probe)
+    t0 = time.perf_counter()
+    run(probe)
+    rate = probe.shape[0] / (time.perf_counter() - t0)
+    sample = int(min(queries.shape[0], max(50_000, rate * 3.0)))
+    t0 = time.perf_counter()
+    run(queries[:sample])
+    sec = time.perf_counter() - t0
+    return {'value': sample / sec, 'unit': 'queries/s', 'cores': nthreads, 'kind': 'reference',
+            'sample': '%d queries of the workload: natinterp3d getInsertionFreeWeightsParallel '
+                      '(%d threads) on the same mesh + scipy W @ values, %.2f s' % (
+                          sample, nthreads, sec)}
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get('RANK', '0'))
+    world = int(os.environ.get('WORLD_SIZE', '1'))
+    local_rank = int(os.environ.get('LOCAL_RANK', '0'))
+
+    if args.impl == 'reference':
+        run_reference(args, rank, world)
+        return
+
+    import torch
+    import natinterp3d_b200 as ni
+    from natinterp3d_b200 import _native
+    from oracle import oracle
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device('cuda', local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        dist.init_process_group('nccl', timeout=datetime.timedelta(seconds=600),
+                                device_id=dev)
+
+    keys, queries, values = make_data(args, rank)
+    t0 = time.perf_counter()
+    interp = ni.Interpolator(keys, device=dev, keep_host_mesh=(rank == 0 and not args.no_cpu_baseline))
+    build_s = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    dm = interp.device_mesh
+    upload_s = time.perf_counter() - t0
+
+    lib = _native.cuda_lib()
+    qd = torch.from_numpy(queries).to(dev)
+    vd = torch.from_numpy(values).to(dev)
+    M = queries.shape[0]
+
+    # correctness gate on a sample before timing: bit-identical to the oracle
+    sample_n = min(M, 20_000)
+    om = oracle.OracleMesh(*interp.mesh_arrays)
+    Wref, stats, _ = om.weights(queries[:sample_n] - interp.centroid, with_stats=True)
+    out_s = dm.interpolate(qd[:sample_n], vd, interp.centroid).cpu().numpy()
+    exact = bool(np.array_equal(out_s, Wref @ values))
+
+    def step():
+        return dm.interpolate(qd, vd, interp.centroid, check=False)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    lib.nif_profile_enable(1)
+    kernel_ms = []
+    with ClockSampler(local_rank) as clocks:
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            step()
+            ph = (ctypes.c_double * 4)()
+            if lib.nif_profile_read(ph) == 0:
+                kernel_ms.append(list(ph))
+        e1.record()
+        torch.cuda.synchronize()
+    lib.nif_profile_enable(0)
+    ms = e0.elapsed_time(e1) / args.steps
+    if dist is not None:
+        t = torch.tensor([ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = M * world / (ms * 1e-3)
+
+    # summary of one extra call (walk steps, large rows), untimed
+    _, summ = dm.interpolate(qd, vd, interp.centroid, return_summary=True)
+
+    # end to end through the public API with host buffers
+    e2e_times = []
+    for i in range(args.e2e_steps + 1):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        out = interp.interpolate(queries, values)
+        e2e_times.append(time.perf_counter() - t0)
+    e2e_sec = float(np.median(e2e_times[1:]))
+    if dist is not None:
+        t = torch.tensor([e2e_sec], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_sec = float(t.item())
+
+    if rank == 0:
+        kms = np.array(kernel_ms) if kernel_ms else np.zeros((1, 4))
+        rows_ms = float(np.mean(kms[:, 1]))
+        fpq = flops_per_query(stats, summ['walk_steps'], M)
+        fused, separate = ctypes.c_double(), ctypes.c_double()
+        lib.nif_measure_fp64_peak(ctypes.byref(fused), ctypes.byref(separate))
+        achieved = fpq * M / (rows_ms * 1e-3) / 1e12 if rows_ms > 0 else None
+        cpu = None if args.no_cpu_baseline else cpu_baseline(interp, queries, values)
+        line = {
+            'metric': METRIC, 'value': value, 'unit': 'queries/s', 'n_gpus': world,
+            'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': ms,
+            'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f64',
+            'data': 'synthetic: seeded uniform keys and queries, N(0,1) float32 values',
+            'config': {
+                'workload': WORKLOAD.format(keys=args.keys, queries=args.queries, dim=args.dim,
+                                            seed=args.seed),
+                'keys': args.keys, 'queries_per_gpu': args.queries, 'D': args.dim,
+                'parallelism': 'replicated mesh, queries sharded' if world > 1 else 'single GPU',
+                'l2': 'inputs larger than L2 (queries %.0f MB, resident mesh %.0f MB)'
+                      % (queries.nbytes / 1e6, dm.nbytes / 1e6),
+                'mesh_build_s': round(build_s, 2), 'mesh_upload_s': round(upload_s, 3),
+                'tets': dm.n_tets, 'bit_identical_to_oracle_on_sample': exact,
+            },
+            'roofline': {
+                'bound': 'fp64', 'kernel': 'k_rows_fast',
+                'achieved': achieved, 'peak': separate.value, 'unit': 'TFLOP/s',
+                'frac': (achieved / separate.value) if achieved and separate.value else None,
+                'peak_fused_fma': fused.value,
+                'peak_note': 'measured on this GPU by nif_measure_fp64_peak: separately rounded '
+                             'DMUL+DADD (the kernels never fuse, for bit parity)',
+                'flops_per_query': fpq, 'kernel_ms': rows_ms,
+                'phase_ms': {'bucketing': float(np.mean(kms[:, 0])), 'rows_fast': rows_ms,
+                             'rows_large': float(np.mean(kms[:, 2])),
+                             'epilogue': float(np.mean(kms[:, 3]))},
+                'traffic': None,
+            },
+            'cpu_baseline': cpu,
+            'e2e': {'value': M * world / e2e_sec, 'unit': 'queries/s',
+                    'h2d_bytes_per_step': int(queries.nbytes + values.nbytes),
+                    'd2h_bytes_per_step': int(out.nbytes)},
+            'gpu_launches': 7 * args.steps,
+            'clocks': clocks.summary(),
+            'summary': {k: int(v) for k, v in summ.items()},
+        }
+        print(json.dumps(line))
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == '__main__':
+    main()

@@ -1,0 +1,180 @@
+/*
+ * natinterp3d_b200 C ABI.
+ *
+ * Two shared libraries sit under the Python package:
+ *   libnif_mesh.so  host-side Delaunay construction (natinterp3d's own
+ *                   constructor) and export of the packed mesh arrays;
+ *   libnif_cuda.so  the sm_100a query kernels.
+ *
+ * Every entry point returns an int status (NIF_OK or a negative code below)
+ * and never aborts or exits the process.  Device pointers (d_*) are plain
+ * CUDA device addresses allocated by the caller; `stream` is a cudaStream_t
+ * (NULL = legacy default stream).  No entry point allocates device memory:
+ * sizes are queried first (nif_dmesh_bytes, nif_query_workspace_bytes) and
+ * the caller passes the buffers in.
+ *
+ * Citations are to natinterp3d's sources (src/natinterp3d/...).
+ */
+#ifndef NATINTERP3D_B200_H
+#define NATINTERP3D_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define NIF_OK 0
+#define NIF_ERR_ARG (-1)        /* invalid argument (natinterp3d: ValueError) */
+#define NIF_ERR_DEGENERATE (-2) /* key set the constructor cannot triangulate */
+#define NIF_ERR_NOMEM (-3)      /* host allocation failed */
+#define NIF_ERR_INTERNAL (-4)   /* inconsistent mesh / internal check failed */
+#define NIF_ERR_OVERFLOW (-5)   /* nnz > INT32_MAX; natinterp3d returns -1 here,
+                                   natural_insertionfree.c:901-912, and Python
+                                   raises OverflowError (natinterp3d_cython.pyx:278-280) */
+#define NIF_ERR_WALK (-6)       /* a point-location walk exceeded its step limit
+                                   (natinterp3d's walk, delaunay.c:398-405, has none) */
+#define NIF_ERR_CUDA (-7)       /* a CUDA runtime call failed */
+#define NIF_ERR_CAPACITY (-8)   /* a query exceeded the large kernel's per-query limits */
+#define NIF_ERR_WORKSPACE (-9)  /* a caller buffer is smaller than the queried size */
+
+/* ---- element types ----------------------------------------------------- */
+#define NIF_F64 0
+#define NIF_F32 1
+
+/* ---- workspace modes --------------------------------------------------- */
+#define NIF_MODE_WEIGHTS 0      /* get_weights: rows are staged, then compacted to CSR */
+#define NIF_MODE_INTERP 1       /* interpolate: rows are reduced against values in place */
+
+/* ======================================================================== */
+/* libnif_mesh.so: host-side construction                                   */
+/* ======================================================================== */
+
+typedef struct nif_mesh nif_mesh;
+
+/* Builds natinterp3d's Delaunay tetrahedralization of n centred keys
+ * ([n][3] float64).  Replaces buildNewMeshAndVertices (natural.h:16,
+ * natural.c:114-118) as called from natinterp3d_cython.pyx:105-106 and
+ * :254-256.  Returns NIF_ERR_DEGENERATE where natinterp3d would exit(1)
+ * (zero or non-finite extent along an axis). */
+int nif_mesh_build(const double *keys_centered, int n, nif_mesh **out);
+
+/* Releases the mesh.  Replaces freeMeshAndVertices (natural.h:18). */
+void nif_mesh_free(nif_mesh *h);
+
+/* Vertex count (n + 4 super-simplex vertices) and tet count of the mesh. */
+int nif_mesh_sizes(const nif_mesh *h, int *n_vertices, int *n_tets);
+
+/* Writes the packed mesh: vxyz [n+4][3] float64 (mesh coordinates, after the
+ * constructor's perturbations, delaunay.c:513-522; super-simplex vertices at
+ * rows n..n+3), tet_v [T][4] int32 (delaunay.h:60), tet_n [T][4] int32
+ * (delaunay.h:64; -1 for NULL).  Tet order is the mesh's tet-list order,
+ * the order natinterp3d packs tets in (natural_insertionfree.c:413-425). */
+int nif_mesh_export(const nif_mesh *h, double *vxyz, int32_t *tet_v, int32_t *tet_n);
+
+/* Degeneracy counters of the constructor (delaunay.c:106-107, 588, 649). */
+int nif_mesh_degeneracies(const nif_mesh *h, int *coplanar, int *cospherical);
+
+/* natinterp3d's own mesh object (for running natinterp3d's CPU query on the
+ * same mesh when checking results). */
+void *nif_mesh_native(const nif_mesh *h);
+
+/* ======================================================================== */
+/* libnif_cuda.so: device-resident mesh and query kernels                   */
+/* ======================================================================== */
+
+typedef struct nif_dmesh nif_dmesh;
+
+/* Size in bytes of the device buffer that holds a resident mesh of
+ * n_vertices (= keys + 4) and n_tets tets: vertices, tets, neighbours,
+ * orientation and mirror flags, cached tet and face circumcentres and the
+ * point-location seed grid.  (natinterp3d keeps the mesh as pointer-linked
+ * structs, delaunay.h:44-70, and re-packs it on first query,
+ * natural_insertionfree.c:397-450.) */
+int nif_dmesh_bytes(int n_vertices, int n_tets, size_t *bytes);
+
+/* Uploads a mesh: derives the resident arrays in d_buf from the packed
+ * arrays written by nif_mesh_export (already copied to the device), and
+ * returns a host handle.  Synchronises `stream`.  The packed input arrays
+ * may be freed afterwards; d_buf must stay alive until nif_dmesh_destroy.
+ * Replaces packMeshSimplices + precomputeOrientSigns
+ * (natural_insertionfree.c:397-476), done once per mesh instead of per call. */
+int nif_dmesh_create(const double *d_vxyz, const int32_t *d_tet_v, const int32_t *d_tet_n,
+                     int n_vertices, int n_tets, void *d_buf, size_t buf_bytes, void *stream,
+                     nif_dmesh **out);
+
+/* Frees the host handle (the device buffer belongs to the caller). */
+void nif_dmesh_destroy(nif_dmesh *m);
+
+/* Seed-grid dimensions and tet/vertex counts:
+ * info = {n_vertices, n_tets, grid_x, grid_y, grid_z, 0, 0, 0}. */
+int nif_dmesh_info(const nif_dmesh *m, int64_t info[8]);
+
+/* Result summary of one query call (host memory). */
+typedef struct {
+    int64_t nnz;            /* non-zeros of the weight matrix */
+    int64_t rows_large;     /* rows that needed the large-capacity kernel */
+    int64_t rows_failed;    /* rows with a non-zero status (left empty) */
+    int64_t rows_outside;   /* queries outside the super-simplex (empty rows) */
+    int64_t walk_steps;     /* total point-location steps */
+    int32_t first_status;   /* status of a failing row, NIF_OK if none */
+    int32_t reserved;
+} nif_summary;
+
+/* Device workspace bytes for M queries in the given mode
+ * (NIF_MODE_WEIGHTS or NIF_MODE_INTERP). */
+int nif_query_workspace_bytes(const nif_dmesh *m, int64_t M, int mode, size_t *bytes);
+
+/* Sibson weights, step 1 of 2.  Queries are M rows of 3 coordinates
+ * (query_dtype NIF_F64 or NIF_F32, C order) in the caller's frame; the key
+ * centroid is subtracted on the device in float64 exactly as
+ * natinterp3d.py:115 does in numpy.  Computes every row into the workspace
+ * and writes d_rowptr (int32[M+1]).  Synchronises `stream` and fills
+ * *summary.  Returns NIF_ERR_OVERFLOW (d_rowptr untouched) when
+ * nnz > INT32_MAX.  Replaces getInsertionFreeWeightsParallel
+ * (natural_insertionfree.h:103-106) up to its row-pointer pass
+ * (natural_insertionfree.c:896-913). */
+int nif_weights_count(const nif_dmesh *m, const void *d_queries, int query_dtype, int64_t M,
+                      const double centroid[3], void *d_ws, size_t ws_bytes, int32_t *d_rowptr,
+                      void *stream, nif_summary *summary);
+
+/* Sibson weights, step 2 of 2: copies the rows staged by nif_weights_count
+ * into CSR arrays d_vals (vals_dtype, nnz) and d_cols (int32, nnz).  Columns
+ * of a row appear in natinterp3d's first-seen order.  Replaces the CSR copy
+ * of natural_insertionfree.c:915-928 (natinterp3d mallocs vals/cols itself). */
+int nif_weights_fill(const nif_dmesh *m, int64_t M, const void *d_ws, size_t ws_bytes,
+                     const int32_t *d_rowptr, void *d_vals, int vals_dtype, int32_t *d_cols,
+                     void *stream);
+
+/* Interpolation without materialising the weights: out[i, :] =
+ * sum_k w_ik values[k, :] for every query, accumulated in row order exactly
+ * as `get_weights(Q) @ values` (natinterp3d.py:131-137, scipy csr_matvecs)
+ * with weights cast to the query dtype and the product in
+ * out_dtype = promote(query_dtype, values_dtype).  values is [N][D] C order.
+ * If summary is non-NULL the call synchronises `stream` and fills it. */
+int nif_interpolate(const nif_dmesh *m, const void *d_queries, int query_dtype, int64_t M,
+                    const double centroid[3], const void *d_values, int values_dtype, int D,
+                    void *d_out, int out_dtype, void *d_ws, size_t ws_bytes, void *stream,
+                    nif_summary *summary);
+
+/* Measurement.  While enabled, every query call records CUDA events on its
+ * stream between its phases; nif_profile_read waits for the last call's
+ * final event and returns the device time in milliseconds of
+ * {query bucketing, shared-memory row kernel, large-row kernel, CSR scan or
+ * epilogue} of that call.  (natinterp3d has no counterpart.) */
+int nif_profile_enable(int on);
+int nif_profile_read(double ms[4]);
+
+/* Measured FP64 throughput of the current device in TFLOP/s (2 flops per
+ * multiply-add pair), with fused multiply-add and with separately rounded
+ * multiply and add -- the latter is the ceiling for the query kernels, which
+ * never fuse.  Allocates 8 bytes of device memory for its duration. */
+int nif_measure_fp64_peak(double *tflops_fused, double *tflops_separate);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* NATINTERP3D_B200_H */

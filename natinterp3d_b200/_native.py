@@ -141,3 +141,65 @@ class HostMesh:
             self.close()
         except Exception:
             pass
+
+
+# --------------------------------------------------------------------------
+# device library
+# --------------------------------------------------------------------------
+NIF_F64 = 0
+NIF_F32 = 1
+NIF_MODE_WEIGHTS = 0
+NIF_MODE_INTERP = 1
+
+
+class Summary(ctypes.Structure):
+    _fields_ = [('nnz', ctypes.c_int64), ('rows_large', ctypes.c_int64),
+                ('rows_failed', ctypes.c_int64), ('rows_outside', ctypes.c_int64),
+                ('walk_steps', ctypes.c_int64), ('first_status', ctypes.c_int32),
+                ('reserved', ctypes.c_int32)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != 'reserved'}
+
+
+# every symbol include/natinterp3d_b200.h declares for libnif_cuda.so, with its ctypes signature
+CUDA_SIGNATURES = {
+    'nif_dmesh_bytes': (c_int, [c_int, c_int, ctypes.POINTER(c_size_t)]),
+    'nif_dmesh_create': (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_int, c_void_p, c_size_t,
+                                 c_void_p, ctypes.POINTER(c_void_p)]),
+    'nif_dmesh_destroy': (None, [c_void_p]),
+    'nif_dmesh_info': (c_int, [c_void_p, ctypes.POINTER(c_int64)]),
+    'nif_query_workspace_bytes': (c_int, [c_void_p, c_int64, c_int, ctypes.POINTER(c_size_t)]),
+    'nif_weights_count': (c_int, [c_void_p, c_void_p, c_int, c_int64, c_double_p, c_void_p,
+                                  c_size_t, c_void_p, c_void_p, ctypes.POINTER(Summary)]),
+    'nif_weights_fill': (c_int, [c_void_p, c_int64, c_void_p, c_size_t, c_void_p, c_void_p, c_int,
+                                 c_void_p, c_void_p]),
+    'nif_interpolate': (c_int, [c_void_p, c_void_p, c_int, c_int64, c_double_p, c_void_p, c_int,
+                                c_int, c_void_p, c_int, c_void_p, c_size_t, c_void_p,
+                                ctypes.POINTER(Summary)]),
+    'nif_profile_enable': (c_int, [c_int]),
+    'nif_profile_read': (c_int, [c_double_p]),
+    'nif_measure_fp64_peak': (c_int, [c_double_p, c_double_p]),
+}
+
+MESH_SIGNATURES = ('nif_mesh_build', 'nif_mesh_free', 'nif_mesh_sizes', 'nif_mesh_export',
+                   'nif_mesh_degeneracies', 'nif_mesh_native')
+
+_cuda_lib = None
+
+
+def cuda_lib():
+    """libnif_cuda.so; raises if it is missing (there is no CPU query path)."""
+    global _cuda_lib
+    if _cuda_lib is None:
+        path = _build.CUDA_SO
+        if not os.path.exists(path):
+            raise RuntimeError('natinterp3d_b200 CUDA library not built (%s); run '
+                               'python -m natinterp3d_b200._build' % path)
+        lib = ctypes.CDLL(path)
+        for name, (res, args) in CUDA_SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _cuda_lib = lib
+    return _cuda_lib

@@ -1,0 +1,1123 @@
+// natinterp3d_b200: sm_100a kernels and the C ABI of libnif_cuda.so
+// (declarations and contracts in include/natinterp3d_b200.h).
+//
+// Query pipeline (one call):
+//   k_bucket / scan / k_scatter   spatial bucketing of the queries (Morton
+//                                 order of a grid over the mesh bounding box),
+//                                 so that concurrently running groups touch
+//                                 nearby tets and the mesh stays in L1/L2;
+//                                 natinterp3d sorts by Morton code for the
+//                                 same reason (natural.c:70-96)
+//   k_rows<fast>                  one group of G lanes per query, scratch in
+//                                 shared memory; rows that exceed its
+//                                 per-query capacities are queued
+//   k_rows<large>                 the queued rows, one warp each, scratch in a
+//                                 global-memory workspace with much larger
+//                                 capacities
+//   then either  count scan + k_compact  (get_weights: CSR)
+//   or the rows were reduced against the values in place (interpolate).
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <new>
+
+#include "natinterp3d_b200.h"
+#include "nif_kernels.cuh"
+
+#define NIF_EXPORT extern "C" __attribute__((visibility("default")))
+
+namespace nif {
+
+// ---------------------------------------------------------------------------
+// capacities
+// ---------------------------------------------------------------------------
+constexpr int FAST_G = 32;
+using FastWS = Workspace<256, 96, 128, 64, 128, 384, FAST_G>;
+constexpr int LARGE_G = 32;
+using LargeWS = Workspace<16384, 4096, 8192, 2048, 8192, 40960, LARGE_G>;
+constexpr int ROW_CAP = FastWS::NBR;  // staged entries per row
+
+constexpr int FAST_BLOCK = 128;       // 4 groups of 32 lanes
+constexpr int LARGE_GROUPS = 64;      // concurrent large-row groups (one warp each)
+constexpr int SCAN_TILE = 2048;
+constexpr int SCAN_THREADS = 256;
+
+inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+// ---------------------------------------------------------------------------
+// per-call device summary (mirrors nif_summary)
+// ---------------------------------------------------------------------------
+struct DevSummary {
+    unsigned long long nnz;
+    unsigned long long rows_large;
+    unsigned long long rows_failed;
+    unsigned long long rows_outside;
+    unsigned long long walk_steps;
+    int first_status;
+    int large_count;  // rows queued for the large kernel
+    unsigned long long arena_used;
+};
+
+// ---------------------------------------------------------------------------
+// resident mesh preparation
+// ---------------------------------------------------------------------------
+
+// validates the packed mesh and converts it to the resident layout
+__global__ void k_prep_vertices(const double *__restrict__ vxyz, int nv, d4 *__restrict__ vtx) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nv; i += gridDim.x * blockDim.x)
+        vtx[i] = d4{vxyz[3 * (size_t)i], vxyz[3 * (size_t)i + 1], vxyz[3 * (size_t)i + 2], 0.0};
+}
+
+__global__ void k_prep_tets(const int32_t *__restrict__ tet_v, const int32_t *__restrict__ tet_n,
+                            int nv, int nt, int4 *__restrict__ tv, int4 *__restrict__ tn,
+                            int *__restrict__ bad) {
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nt; t += gridDim.x * blockDim.x) {
+        int4 p = make_int4(tet_v[4 * (size_t)t], tet_v[4 * (size_t)t + 1], tet_v[4 * (size_t)t + 2],
+                           tet_v[4 * (size_t)t + 3]);
+        int4 n = make_int4(tet_n[4 * (size_t)t], tet_n[4 * (size_t)t + 1], tet_n[4 * (size_t)t + 2],
+                           tet_n[4 * (size_t)t + 3]);
+        bool ok = true;
+        for (int j = 0; j < 4; j++) {
+            ok = ok && comp(p, j) >= 0 && comp(p, j) < nv;
+            ok = ok && comp(n, j) >= -1 && comp(n, j) < nt;
+        }
+        if (!ok) {
+            atomicExch(bad, 1);
+            p = make_int4(0, 0, 0, 0);
+            n = make_int4(-1, -1, -1, -1);
+        }
+        tv[t] = p;
+        tn[t] = n;
+    }
+}
+
+// orientation flag, mirror slots, tet and face circumcentres
+__global__ void k_prep_geometry(MeshView M, uint32_t *__restrict__ tinfo, d4 *__restrict__ tcc,
+                                d4 *__restrict__ fcc, int *__restrict__ bad) {
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < M.nt; t += gridDim.x * blockDim.x) {
+        const int4 p = M.tv[t];
+        const int4 n = M.tn[t];
+        const dv3 P0 = vload(M, p.x), P1 = vload(M, p.y), P2 = vload(M, p.z), P3 = vload(M, p.w);
+        // natinterp3d recomputes this sign on every call (natural_insertionfree.c:457-476)
+        uint32_t info = orient_fast(P0, P1, P2, P3) > 0 ? 1u : 0u;
+        for (int j = 0; j < 4; j++) {
+            const int nb = comp(n, j);
+            int jm = 0;
+            if (nb >= 0) {
+                const int4 nn = M.tn[nb];
+                jm = -1;
+                for (int k = 0; k < 4; k++)
+                    if (comp(nn, k) == t && jm < 0) jm = k;
+                if (jm < 0) {
+                    atomicExch(bad, 2);
+                    jm = 0;
+                }
+            }
+            info |= (uint32_t)jm << (8 + 2 * j);
+        }
+        tinfo[t] = info;
+        const dv3 c = tet_cc(P0, P1, P2, P3);
+        tcc[t] = d4{c.x, c.y, c.z, 0.0};
+        // face opposite p[i], remaining vertices in ascending slot order
+        // (natural_insertionfree.c:649-652)
+        const dv3 f0 = tri_cc(P1, P2, P3);
+        const dv3 f1 = tri_cc(P0, P2, P3);
+        const dv3 f2 = tri_cc(P0, P1, P3);
+        const dv3 f3 = tri_cc(P0, P1, P2);
+        fcc[4 * (size_t)t + 0] = d4{f0.x, f0.y, f0.z, 0.0};
+        fcc[4 * (size_t)t + 1] = d4{f1.x, f1.y, f1.z, 0.0};
+        fcc[4 * (size_t)t + 2] = d4{f2.x, f2.y, f2.z, 0.0};
+        fcc[4 * (size_t)t + 3] = d4{f3.x, f3.y, f3.z, 0.0};
+    }
+}
+
+// bounding box of the data vertices: per-block partials (6 doubles per block)
+__global__ void k_bbox_partial(const d4 *__restrict__ vtx, int n, double *__restrict__ part) {
+    double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const d4 v = vtx[i];
+        lo[0] = fmin(lo[0], v.x); lo[1] = fmin(lo[1], v.y); lo[2] = fmin(lo[2], v.z);
+        hi[0] = fmax(hi[0], v.x); hi[1] = fmax(hi[1], v.y); hi[2] = fmax(hi[2], v.z);
+    }
+    __shared__ double s[6][256];
+    for (int a = 0; a < 3; a++) {
+        s[a][threadIdx.x] = lo[a];
+        s[3 + a][threadIdx.x] = hi[a];
+    }
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w)
+            for (int a = 0; a < 3; a++) {
+                s[a][threadIdx.x] = fmin(s[a][threadIdx.x], s[a][threadIdx.x + w]);
+                s[3 + a][threadIdx.x] = fmax(s[3 + a][threadIdx.x], s[3 + a][threadIdx.x + w]);
+            }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        for (int a = 0; a < 6; a++) part[6 * blockIdx.x + a] = s[a][0];
+}
+
+// Seed grid, built coarse to fine: the tet of every cell of level k is found
+// by walking from its parent cell's tet to the cell centre.
+__global__ void k_seed_level(MeshView M, int dx, int dy, int dz, int pdx, int pdy, int pdz,
+                             const int *__restrict__ parent, int *__restrict__ out, int *__restrict__ bad) {
+    const int ncell = dx * dy * dz;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < ncell; c += gridDim.x * blockDim.x) {
+        const int x = c % dx, y = (c / dx) % dy, z = c / (dx * dy);
+        int t = 0;
+        if (parent) {
+            const int px = (pdx == dx) ? x : x >> 1;
+            const int py = (pdy == dy) ? y : y >> 1;
+            const int pz = (pdz == dz) ? z : z >> 1;
+            t = parent[(pz * pdy + py) * pdx + px];
+        }
+        // centre of the cell: the finest grid has gdim cells of 1/ginv per axis,
+        // this level has d cells of gdim/(d*ginv)
+        const dv3 q = mk(M.glo[0] + (x + 0.5) * (double)M.gdim[0] / (dx * M.ginv[0]),
+                         M.glo[1] + (y + 0.5) * (double)M.gdim[1] / (dy * M.ginv[1]),
+                         M.glo[2] + (z + 0.5) * (double)M.gdim[2] / (dz * M.ginv[2]));
+        const int t0 = t;
+        for (int step = 0; step < (1 << 22); step++) {
+            const int4 p = M.tv[t];
+            int f = 0;
+            for (; f < 4; f++) {
+                const dv3 v1 = vload(M, comp(p, face_vslot(f, 0)));
+                const dv3 v2 = vload(M, comp(p, face_vslot(f, 1)));
+                const dv3 v3 = vload(M, comp(p, face_vslot(f, 2)));
+                if (orient_fast(v1, v2, v3, q) < 0) break;
+            }
+            if (f == 4) break;
+            const int nb = comp(M.tn[t], f);
+            if (nb < 0) break;  // centre outside the super-simplex: keep the last tet
+            t = nb;
+            if (step == (1 << 22) - 1) t = t0;  // no convergence: keep the parent's seed
+        }
+        out[c] = t;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// query bucketing
+// ---------------------------------------------------------------------------
+template <class QT>
+__device__ __forceinline__ dv3 load_query(const QT *__restrict__ Q, int64_t i, const double *cen) {
+    // natinterp3d.py:115: np.ascontiguousarray(Q, float64) - centroid
+    return dv3{fsub((double)Q[3 * i], cen[0]), fsub((double)Q[3 * i + 1], cen[1]),
+               fsub((double)Q[3 * i + 2], cen[2])};
+}
+
+struct Centroid {
+    double c[3];
+};
+
+__device__ __forceinline__ unsigned spread3(unsigned v) {  // 10 bits -> every third bit
+    v &= 0x3ffu;
+    v = (v | (v << 16)) & 0x030000ffu;
+    v = (v | (v << 8)) & 0x0300f00fu;
+    v = (v | (v << 4)) & 0x030c30c3u;
+    v = (v | (v << 2)) & 0x09249249u;
+    return v;
+}
+
+template <class QT>
+__global__ void k_bucket(const QT *__restrict__ Q, int64_t M, Centroid cen, MeshView mv, int bits,
+                         int *__restrict__ bucket, int *__restrict__ bcount) {
+    const double scale = (double)(1 << bits);
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < M;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const dv3 q = load_query(Q, i, cen.c);
+        const double c[3] = {q.x, q.y, q.z};
+        unsigned code = 0;
+        for (int a = 0; a < 3; a++) {
+            double f = (c[a] - mv.glo[a]) * mv.ginv[a] / (double)mv.gdim[a] * scale;
+            int k = (f >= 0.0) ? (f < scale ? (int)f : (1 << bits) - 1) : 0;
+            code |= spread3((unsigned)k) << a;
+        }
+        bucket[i] = (int)code;
+        atomicAdd(&bcount[code], 1);
+    }
+}
+
+__global__ void k_scatter(const int *__restrict__ bucket, int64_t M, int *__restrict__ cursor,
+                          int *__restrict__ order) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < M;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const int pos = atomicAdd(&cursor[bucket[i]], 1);
+        order[pos] = (int)i;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// exclusive scan (three passes): int32 input, OutT output, optional total
+// ---------------------------------------------------------------------------
+template <class OutT>
+__global__ void k_scan_reduce(const int *__restrict__ in, int64_t n, OutT *__restrict__ bsum) {
+    __shared__ OutT s[SCAN_THREADS];
+    const int64_t base = (int64_t)blockIdx.x * SCAN_TILE;
+    OutT acc = 0;
+    for (int k = threadIdx.x; k < SCAN_TILE; k += SCAN_THREADS) {
+        const int64_t i = base + k;
+        if (i < n) acc += (OutT)in[i];
+    }
+    s[threadIdx.x] = acc;
+    __syncthreads();
+    for (int w = SCAN_THREADS / 2; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w) s[threadIdx.x] += s[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) bsum[blockIdx.x] = s[0];
+}
+
+// single block: exclusive scan of the block sums in place, total to *total
+template <class OutT>
+__global__ void k_scan_blocks(OutT *__restrict__ bsum, int nb, OutT *__restrict__ total) {
+    __shared__ OutT s[SCAN_THREADS];
+    __shared__ OutT carry;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    for (int b0 = 0; b0 < nb; b0 += SCAN_THREADS) {
+        const int i = b0 + threadIdx.x;
+        const OutT v = (i < nb) ? bsum[i] : 0;
+        s[threadIdx.x] = v;
+        __syncthreads();
+        for (int w = 1; w < SCAN_THREADS; w <<= 1) {
+            const OutT add = ((int)threadIdx.x >= w) ? s[threadIdx.x - w] : 0;
+            __syncthreads();
+            s[threadIdx.x] += add;
+            __syncthreads();
+        }
+        if (i < nb) bsum[i] = carry + s[threadIdx.x] - v;
+        __syncthreads();
+        if (threadIdx.x == SCAN_THREADS - 1) carry += s[threadIdx.x];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0 && total) *total = carry;
+}
+
+template <class OutT>
+__global__ void k_scan_apply(const int *__restrict__ in, int64_t n, const OutT *__restrict__ bsum,
+                             OutT *__restrict__ out) {
+    __shared__ OutT s[SCAN_THREADS];
+    constexpr int PER = SCAN_TILE / SCAN_THREADS;
+    const int64_t base = (int64_t)blockIdx.x * SCAN_TILE + (int64_t)threadIdx.x * PER;
+    OutT v[PER];
+    OutT acc = 0;
+    for (int k = 0; k < PER; k++) {
+        const int64_t i = base + k;
+        v[k] = (i < n) ? (OutT)in[i] : 0;
+        acc += v[k];
+    }
+    s[threadIdx.x] = acc;
+    __syncthreads();
+    for (int w = 1; w < SCAN_THREADS; w <<= 1) {
+        const OutT add = ((int)threadIdx.x >= w) ? s[threadIdx.x - w] : 0;
+        __syncthreads();
+        s[threadIdx.x] += add;
+        __syncthreads();
+    }
+    OutT run = bsum[blockIdx.x] + s[threadIdx.x] - acc;
+    for (int k = 0; k < PER; k++) {
+        const int64_t i = base + k;
+        if (i < n) out[i] = run;
+        run += v[k];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// row sinks
+// ---------------------------------------------------------------------------
+
+// get_weights: rows staged per original row index, compacted afterwards
+struct StageSink {
+    int *__restrict__ cnt;          // [M]
+    int64_t *__restrict__ src;      // [M] first staged entry of the row
+    int *__restrict__ cols;         // [M*ROW_CAP + arena]
+    double *__restrict__ vals;      // [M*ROW_CAP + arena]
+    int64_t arena_base;             // = M*ROW_CAP
+    int64_t arena_cap;
+    DevSummary *sum;
+
+    template <int G, class W>
+    __device__ __forceinline__ void emit(int64_t i, int nnb, const W &ws, const Grp<G> &g,
+                                         bool large) {
+        int64_t o = i * ROW_CAP;
+        if (large) {
+            unsigned long long a = 0;
+            if (g.lane == 0) a = atomicAdd(&sum->arena_used, (unsigned long long)nnb);
+            a = __shfl_sync(g.mask, a, 0, G);
+            if ((int64_t)(a + nnb) > arena_cap) {
+                if (g.lane == 0) {
+                    cnt[i] = 0;
+                    src[i] = 0;
+                    atomicAdd(&sum->rows_failed, 1ull);
+                    atomicCAS(&sum->first_status, 0, NIF_ERR_CAPACITY);
+                }
+                return;
+            }
+            o = arena_base + (int64_t)a;
+        }
+        for (int s = g.lane; s < nnb; s += G) {
+            cols[o + s] = ws.nbr_vid[s];
+            vals[o + s] = ws.w[s];
+        }
+        if (g.lane == 0) {
+            cnt[i] = nnb;
+            src[i] = o;
+        }
+    }
+    __device__ __forceinline__ void empty(int64_t i, int lane) {
+        if (lane == 0) {
+            cnt[i] = 0;
+            src[i] = 0;
+        }
+    }
+};
+
+template <class T> struct Arith;
+template <> struct Arith<double> {
+    __device__ static double mul(double a, double b) { return __dmul_rn(a, b); }
+    __device__ static double add(double a, double b) { return __dadd_rn(a, b); }
+};
+template <> struct Arith<float> {
+    __device__ static float mul(float a, float b) { return __fmul_rn(a, b); }
+    __device__ static float add(float a, float b) { return __fadd_rn(a, b); }
+};
+
+// interpolate: out[i, :] = sum over the row of (CT)(WT)w * (CT)values[col, :],
+// accumulated in stored order from zero (scipy csr_matvec / csr_matvecs)
+template <class WT, class VT, class CT>
+struct InterpSink {
+    const VT *__restrict__ values;  // [N][D]
+    CT *__restrict__ out;           // [M][D]
+    int D;
+
+    template <int G, class W>
+    __device__ __forceinline__ void emit(int64_t i, int nnb, W &ws, const Grp<G> &g, bool) {
+        CT *o = out + i * (int64_t)D;
+        if (nnb == 0) {
+            for (int d = g.lane; d < D; d += G) o[d] = (CT)0;
+            return;
+        }
+        // products staged in the (now free) term buffer, dc columns at a time
+        double *buf = ws.u.b.terms;
+        const int dc = max(1, min(D, W::TERMS / nnb));
+        for (int d0 = 0; d0 < D; d0 += dc) {
+            const int nd = min(dc, D - d0);
+            g.sync();
+            for (int k = g.lane; k < nnb * nd; k += G) {
+                const int s = k / nd, d = k - s * nd;
+                const CT w = (CT)(WT)ws.w[s];
+                const CT x = (CT)values[(int64_t)ws.nbr_vid[s] * D + d0 + d];
+                buf[k] = (double)Arith<CT>::mul(w, x);
+            }
+            g.sync();
+            for (int d = g.lane; d < nd; d += G) {
+                CT acc = (CT)0;
+                for (int s = 0; s < nnb; s++) acc = Arith<CT>::add(acc, (CT)buf[s * nd + d]);
+                o[d0 + d] = acc;
+            }
+        }
+        g.sync();
+    }
+    __device__ __forceinline__ void empty(int64_t i, int lane) {
+        CT *o = out + i * (int64_t)D;
+        if (lane == 0)
+            for (int d = 0; d < D; d++) o[d] = (CT)0;
+    }
+};
+
+// ---------------------------------------------------------------------------
+// row kernels
+// ---------------------------------------------------------------------------
+struct LargeQueue {
+    int *__restrict__ list;  // [M]
+};
+
+template <int G>
+__device__ __forceinline__ void record(DevSummary *sum, const RowInfo &r, int lane) {
+    if (lane != 0) return;
+    if (r.outside) atomicAdd(&sum->rows_outside, 1ull);
+}
+
+// fast path: shared-memory scratch, rows in bucket order
+template <class QT, class Sink>
+__global__ void __launch_bounds__(FAST_BLOCK) k_rows_fast(MeshView M, const QT *__restrict__ Q,
+                                                          Centroid cen, const int *__restrict__ order,
+                                                          int64_t nrows, Sink sink, LargeQueue lq,
+                                                          DevSummary *sum) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    constexpr int G = FAST_G;
+    constexpr int GPB = FAST_BLOCK / G;
+    Grp<G> g;
+    FastWS &ws = reinterpret_cast<FastWS *>(smem)[threadIdx.x / G];
+    const int64_t gid = (int64_t)blockIdx.x * GPB + threadIdx.x / G;
+    const int64_t ng = (int64_t)gridDim.x * GPB;
+    unsigned long long steps = 0;
+    for (int64_t s = gid; s < nrows; s += ng) {
+        const int64_t i = order[s];
+        const dv3 q = load_query(Q, i, cen.c);
+        const RowInfo r = sibson_row<G>(M, q, ws, g);
+        steps += r.steps;
+        if (r.status == ST_CAPACITY) {
+            if (g.lane == 0) {
+                const int slot = atomicAdd(&sum->large_count, 1);
+                lq.list[slot] = (int)i;
+            }
+        } else {
+            if (r.status != ST_OK && g.lane == 0) {
+                atomicAdd(&sum->rows_failed, 1ull);
+                atomicCAS(&sum->first_status, 0, NIF_ERR_WALK);
+            }
+            record<G>(sum, r, g.lane);
+            sink.template emit<G>(i, r.status == ST_OK ? r.nnb : 0, ws, g, false);
+        }
+        g.sync();
+    }
+    if (g.lane == 0 && steps) atomicAdd(&sum->walk_steps, steps);
+}
+
+// large path: one warp per queued row, scratch in global memory
+template <class QT, class Sink>
+__global__ void __launch_bounds__(32) k_rows_large(MeshView M, const QT *__restrict__ Q, Centroid cen,
+                                                   LargeQueue lq, Sink sink, LargeWS *__restrict__ wsv,
+                                                   DevSummary *sum) {
+    constexpr int G = LARGE_G;
+    Grp<G> g;
+    LargeWS &ws = wsv[blockIdx.x];
+    const int nq = sum->large_count;
+    unsigned long long steps = 0;
+    for (int j = blockIdx.x; j < nq; j += gridDim.x) {
+        const int64_t i = lq.list[j];
+        const dv3 q = load_query(Q, i, cen.c);
+        const RowInfo r = sibson_row<G>(M, q, ws, g);
+        steps += r.steps;
+        if (g.lane == 0) atomicAdd(&sum->rows_large, 1ull);
+        if (r.status != ST_OK) {
+            if (g.lane == 0) {
+                atomicAdd(&sum->rows_failed, 1ull);
+                atomicCAS(&sum->first_status, 0,
+                          r.status == ST_WALK ? NIF_ERR_WALK : NIF_ERR_CAPACITY);
+            }
+            sink.template emit<G>(i, 0, ws, g, true);
+        } else {
+            record<G>(sum, r, g.lane);
+            sink.template emit<G>(i, r.nnb, ws, g, true);
+        }
+        g.sync();
+    }
+    if (g.lane == 0 && steps) atomicAdd(&sum->walk_steps, steps);
+}
+
+// CSR compaction: 16 lanes per row
+template <class VT>
+__global__ void k_compact(int64_t M, const int *__restrict__ cnt, const int64_t *__restrict__ src,
+                          const int *__restrict__ scols, const double *__restrict__ svals,
+                          const int32_t *__restrict__ rowptr, int32_t *__restrict__ cols,
+                          VT *__restrict__ vals) {
+    const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t u = tid; u < M * 16; u += stride) {
+        const int64_t i = u >> 4;
+        const int l = (int)(u & 15);
+        const int n = cnt[i];
+        const int64_t s = src[i];
+        const int64_t d = rowptr[i];
+        for (int k = l; k < n; k += 16) {
+            cols[d + k] = scols[s + k];
+            vals[d + k] = (VT)svals[s + k];
+        }
+    }
+}
+
+__global__ void k_rowptr32(const int64_t *__restrict__ off, int64_t M, int64_t total,
+                           int32_t *__restrict__ rowptr) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i <= M;
+         i += (int64_t)gridDim.x * blockDim.x)
+        rowptr[i] = (int32_t)(i < M ? off[i] : total);
+}
+
+// FP64 throughput probe: 8 independent chains per thread of either
+// separately rounded multiply and add (2 instructions, 2 flops) or fused
+// multiply-add (1 instruction, 2 flops).
+template <bool FUSED>
+__global__ void k_fp64_peak(double *out, int iters, double b, double c) {
+    double a[8];
+    for (int k = 0; k < 8; k++) a[k] = threadIdx.x * 1e-9 + k;
+    for (int i = 0; i < iters; i++) {
+#pragma unroll
+        for (int k = 0; k < 8; k++) a[k] = FUSED ? __fma_rn(a[k], b, c) : __dadd_rn(__dmul_rn(a[k], b), c);
+    }
+    double r = 0.0;
+    for (int k = 0; k < 8; k++) r += a[k];
+    if (r == 12345.678) out[0] = r;  // keeps the chains live
+}
+
+}  // namespace nif
+
+using namespace nif;
+
+// ===========================================================================
+// host side
+// ===========================================================================
+struct nif_dmesh {
+    MeshView view;
+    int n_vertices, n_tets;
+    int device;
+    int num_sms;
+    size_t bytes;
+};
+
+namespace {
+
+struct Carve {
+    unsigned char *base;
+    size_t off;
+    size_t cap;
+    bool ok;
+    template <class T>
+    T *take(size_t count) {
+        off = align_up(off, 256);
+        T *p = reinterpret_cast<T *>(base + off);
+        off += count * sizeof(T);
+        if (off > cap) ok = false;
+        return p;
+    }
+};
+
+inline cudaStream_t S(void *s) { return reinterpret_cast<cudaStream_t>(s); }
+
+inline int cuda_rc(cudaError_t e) { return e == cudaSuccess ? NIF_OK : NIF_ERR_CUDA; }
+
+#define NIF_CUDA(call)                                  \
+    do {                                                \
+        cudaError_t e_ = (call);                        \
+        if (e_ != cudaSuccess) return NIF_ERR_CUDA;     \
+    } while (0)
+
+size_t grid_cells_max(int n_vertices) {
+    size_t n = n_vertices > 4 ? (size_t)(n_vertices - 4) : 1;
+    size_t c = 1;
+    while (c < n && c < ((size_t)1 << 24)) c <<= 1;
+    return c;
+}
+
+struct MeshLayout {
+    d4 *vtx;
+    int4 *tv, *tn;
+    uint32_t *tinfo;
+    d4 *tcc, *fcc;
+    int *grid_a, *grid_b;  // ping-pong seed levels
+    double *bbox_part;
+    int *flag;
+};
+
+MeshLayout carve_mesh(Carve &c, int nv, int nt) {
+    MeshLayout L;
+    L.vtx = c.take<d4>(nv);
+    L.tv = c.take<int4>(nt);
+    L.tn = c.take<int4>(nt);
+    L.tinfo = c.take<uint32_t>(nt);
+    L.tcc = c.take<d4>(nt);
+    L.fcc = c.take<d4>(4 * (size_t)nt);
+    const size_t gm = grid_cells_max(nv);
+    L.grid_a = c.take<int>(gm);
+    L.grid_b = c.take<int>(gm);
+    L.bbox_part = c.take<double>(6 * 256);
+    L.flag = c.take<int>(4);
+    return L;
+}
+
+int blocks_for(int64_t n, int threads, int cap = 148 * 32) {
+    int64_t b = (n + threads - 1) / threads;
+    if (b < 1) b = 1;
+    if (b > cap) b = cap;
+    return (int)b;
+}
+
+// query workspace layout
+struct QueryLayout {
+    DevSummary *sum;
+    int *bucket, *bcount, *order, *large_list;
+    int64_t *scan_bsum;     // block sums for the scans
+    int64_t *scan_total;
+    LargeWS *large_ws;
+    // weights mode only
+    int *cnt;
+    int64_t *src, *off64;
+    int *scols;
+    double *svals;
+    int64_t arena_cap;
+};
+
+int bucket_bits(int64_t M) {
+    int b = 1;
+    while (b < 10 && ((int64_t)1 << (3 * (b + 1))) <= M / 2) b++;
+    return b;
+}
+
+QueryLayout carve_query(Carve &c, int64_t M, int mode) {
+    QueryLayout L{};
+    const int bits = bucket_bits(M);
+    const int64_t nbk = (int64_t)1 << (3 * bits);
+    const int64_t mscan = M > nbk ? M : nbk;
+    L.sum = c.take<DevSummary>(1);
+    L.bucket = c.take<int>(M > 0 ? M : 1);
+    L.bcount = c.take<int>(nbk + 1);
+    L.order = c.take<int>(M > 0 ? M : 1);
+    L.large_list = c.take<int>(M > 0 ? M : 1);
+    L.scan_bsum = c.take<int64_t>((mscan + SCAN_TILE - 1) / SCAN_TILE + 1);
+    L.scan_total = c.take<int64_t>(1);
+    L.large_ws = c.take<LargeWS>(LARGE_GROUPS);
+    if (mode == NIF_MODE_WEIGHTS) {
+        L.arena_cap = (int64_t)1 << 22;
+        const int64_t stage = M * ROW_CAP + L.arena_cap;
+        L.cnt = c.take<int>(M > 0 ? M : 1);
+        L.src = c.take<int64_t>(M > 0 ? M : 1);
+        L.off64 = c.take<int64_t>(M + 1);
+        L.scols = c.take<int>(stage);
+        L.svals = c.take<double>(stage);
+    }
+    return L;
+}
+
+template <class OutT>
+void launch_scan(const int *in, int64_t n, OutT *bsum, OutT *total, OutT *out, cudaStream_t st) {
+    const int64_t nb = (n + SCAN_TILE - 1) / SCAN_TILE;
+    if (nb == 0) {
+        k_scan_blocks<OutT><<<1, SCAN_THREADS, 0, st>>>(bsum, 0, total);
+        return;
+    }
+    k_scan_reduce<OutT><<<(unsigned)nb, SCAN_THREADS, 0, st>>>(in, n, bsum);
+    k_scan_blocks<OutT><<<1, SCAN_THREADS, 0, st>>>(bsum, (int)nb, total);
+    k_scan_apply<OutT><<<(unsigned)nb, SCAN_THREADS, 0, st>>>(in, n, bsum, out);
+}
+
+int fast_grid(const nif_dmesh *m, int64_t M) {
+    static int per_sm = -1;
+    if (per_sm < 0) {
+        per_sm = 0;
+        // occupancy is identical for every instantiation (same block and smem)
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+            &per_sm, k_rows_fast<double, StageSink>, FAST_BLOCK,
+            (FAST_BLOCK / FAST_G) * sizeof(FastWS));
+        if (per_sm < 1) per_sm = 1;
+    }
+    const int64_t groups = (M + 0) / 1;
+    int64_t blocks = (groups + (FAST_BLOCK / FAST_G) - 1) / (FAST_BLOCK / FAST_G);
+    const int64_t cap = (int64_t)per_sm * m->num_sms;
+    if (blocks > cap) blocks = cap;
+    if (blocks < 1) blocks = 1;
+    return (int)blocks;
+}
+
+template <class Kern>
+int set_smem(Kern k, size_t bytes) {
+    return cuda_rc(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+}
+
+// Optional phase timing (nif_profile_enable / nif_profile_read): events
+// recorded on the launching stream between the phases of a query call.
+constexpr int PROF_EVENTS = 5;  // start | bucketing | fast rows | large rows | finish
+struct Profiler {
+    bool on = false;
+    bool created = false;
+    int recorded = 0;
+    cudaEvent_t ev[PROF_EVENTS];
+};
+Profiler g_prof;
+
+inline void prof_mark(int k, cudaStream_t st) {
+    if (!g_prof.on) return;
+    if (!g_prof.created) {
+        for (int i = 0; i < PROF_EVENTS; i++) cudaEventCreate(&g_prof.ev[i]);
+        g_prof.created = true;
+    }
+    cudaEventRecord(g_prof.ev[k], st);
+    if (k + 1 > g_prof.recorded) g_prof.recorded = k + 1;
+    if (k == 0) g_prof.recorded = 1;
+}
+
+// bucket the queries (writes L.order); positions fit int32 because M < 2^31
+template <class QT>
+void run_bucketing(const nif_dmesh *m, const QT *Q, int64_t M, const Centroid &cen,
+                   const QueryLayout &L, cudaStream_t st) {
+    const int bits = bucket_bits(M);
+    const int64_t nbk = (int64_t)1 << (3 * bits);
+    prof_mark(0, st);
+    cudaMemsetAsync(L.bcount, 0, sizeof(int) * (nbk + 1), st);
+    k_bucket<QT><<<blocks_for(M, 256), 256, 0, st>>>(Q, M, cen, m->view, bits, L.bucket, L.bcount);
+    // in-place exclusive scan: bucket starts become the scatter cursors
+    launch_scan<int>(L.bcount, nbk, reinterpret_cast<int *>(L.scan_bsum),
+                     reinterpret_cast<int *>(L.scan_total), L.bcount, st);
+    k_scatter<<<blocks_for(M, 256), 256, 0, st>>>(L.bucket, M, L.bcount, L.order);
+    prof_mark(1, st);
+}
+
+template <class QT, class Sink>
+void run_rows(const nif_dmesh *m, const QT *Q, int64_t M, const Centroid &cen, const QueryLayout &L,
+              const Sink &sink, cudaStream_t st) {
+    const size_t smem = (FAST_BLOCK / FAST_G) * sizeof(FastWS);
+    k_rows_fast<QT, Sink><<<fast_grid(m, M), FAST_BLOCK, smem, st>>>(
+        m->view, Q, cen, L.order, M, sink, LargeQueue{L.large_list}, L.sum);
+    prof_mark(2, st);
+    k_rows_large<QT, Sink><<<LARGE_GROUPS, 32, 0, st>>>(m->view, Q, cen, LargeQueue{L.large_list},
+                                                        sink, L.large_ws, L.sum);
+    prof_mark(3, st);
+}
+
+__global__ void k_rowptr_guarded(const int64_t *__restrict__ off, int64_t M,
+                                 const int64_t *__restrict__ total, int32_t *__restrict__ rowptr) {
+    const int64_t tot = *total;
+    if (tot > INT32_MAX) return;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i <= M;
+         i += (int64_t)gridDim.x * blockDim.x)
+        rowptr[i] = (int32_t)(i < M ? off[i] : tot);
+}
+
+int read_summary(const QueryLayout &L, cudaStream_t st, nif_summary *out, int64_t *total) {
+    DevSummary d;
+    int64_t tot = 0;
+    NIF_CUDA(cudaMemcpyAsync(&d, L.sum, sizeof(d), cudaMemcpyDeviceToHost, st));
+    if (total) NIF_CUDA(cudaMemcpyAsync(&tot, L.scan_total, sizeof(tot), cudaMemcpyDeviceToHost, st));
+    NIF_CUDA(cudaStreamSynchronize(st));
+    NIF_CUDA(cudaGetLastError());
+    if (out) {
+        out->nnz = total ? tot : 0;
+        out->rows_large = (int64_t)d.rows_large;
+        out->rows_failed = (int64_t)d.rows_failed;
+        out->rows_outside = (int64_t)d.rows_outside;
+        out->walk_steps = (int64_t)d.walk_steps;
+        out->first_status = d.first_status;
+        out->reserved = 0;
+    }
+    if (total) *total = tot;
+    return NIF_OK;
+}
+
+int check_query_args(const nif_dmesh *m, const void *q, int qdt, int64_t M, const double *cen,
+                     const void *ws) {
+    if (!m || !cen || M < 0 || M > (int64_t)INT32_MAX) return NIF_ERR_ARG;
+    if (qdt != NIF_F64 && qdt != NIF_F32) return NIF_ERR_ARG;
+    if (M > 0 && (!q || !ws)) return NIF_ERR_ARG;
+    if (ws && reinterpret_cast<uintptr_t>(ws) % 256 != 0) return NIF_ERR_ARG;
+    return NIF_OK;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// exported API
+// ---------------------------------------------------------------------------
+NIF_EXPORT int nif_dmesh_bytes(int n_vertices, int n_tets, size_t *bytes) {
+    if (!bytes || n_vertices < 5 || n_tets < 1) return NIF_ERR_ARG;
+    Carve c{nullptr, 0, (size_t)-1, true};
+    carve_mesh(c, n_vertices, n_tets);
+    *bytes = align_up(c.off, 256);
+    return NIF_OK;
+}
+
+NIF_EXPORT int nif_dmesh_create(const double *d_vxyz, const int32_t *d_tet_v,
+                                const int32_t *d_tet_n, int n_vertices, int n_tets, void *d_buf,
+                                size_t buf_bytes, void *stream, nif_dmesh **out) {
+    if (!out) return NIF_ERR_ARG;
+    *out = nullptr;
+    if (!d_vxyz || !d_tet_v || !d_tet_n || !d_buf || n_vertices < 5 || n_tets < 1)
+        return NIF_ERR_ARG;
+    if (reinterpret_cast<uintptr_t>(d_buf) % 256 != 0) return NIF_ERR_ARG;
+    size_t need = 0;
+    nif_dmesh_bytes(n_vertices, n_tets, &need);
+    if (buf_bytes < need) return NIF_ERR_WORKSPACE;
+    cudaStream_t st = S(stream);
+    Carve c{reinterpret_cast<unsigned char *>(d_buf), 0, buf_bytes, true};
+    MeshLayout L = carve_mesh(c, n_vertices, n_tets);
+
+    nif_dmesh *h = new (std::nothrow) nif_dmesh();
+    if (!h) return NIF_ERR_NOMEM;
+    h->n_vertices = n_vertices;
+    h->n_tets = n_tets;
+    h->bytes = need;
+    if (cudaGetDevice(&h->device) != cudaSuccess ||
+        cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, h->device) != cudaSuccess) {
+        delete h;
+        return NIF_ERR_CUDA;
+    }
+    MeshView &V = h->view;
+    V.vtx = L.vtx;
+    V.tv = L.tv;
+    V.tn = L.tn;
+    V.tinfo = L.tinfo;
+    V.tcc = L.tcc;
+    V.fcc = L.fcc;
+    V.n = n_vertices - 4;
+    V.nv = n_vertices;
+    V.nt = n_tets;
+
+    int rc = NIF_OK;
+    do {
+        if (cudaMemsetAsync(L.flag, 0, 4 * sizeof(int), st) != cudaSuccess) { rc = NIF_ERR_CUDA; break; }
+        k_prep_vertices<<<blocks_for(n_vertices, 256), 256, 0, st>>>(d_vxyz, n_vertices, L.vtx);
+        k_prep_tets<<<blocks_for(n_tets, 256), 256, 0, st>>>(d_tet_v, d_tet_n, n_vertices, n_tets,
+                                                             L.tv, L.tn, L.flag);
+        k_prep_geometry<<<blocks_for(n_tets, 128), 128, 0, st>>>(V, L.tinfo, L.tcc, L.fcc, L.flag);
+        const int nbb = blocks_for(V.n, 256, 256);
+        k_bbox_partial<<<nbb, 256, 0, st>>>(L.vtx, V.n, L.bbox_part);
+        double part[6 * 256];
+        int flag[4];
+        if (cudaMemcpyAsync(part, L.bbox_part, sizeof(double) * 6 * nbb, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+            cudaMemcpyAsync(flag, L.flag, sizeof(flag), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+            cudaStreamSynchronize(st) != cudaSuccess) {
+            rc = NIF_ERR_CUDA;
+            break;
+        }
+        if (flag[0]) { rc = NIF_ERR_INTERNAL; break; }
+        double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+        for (int b = 0; b < nbb; b++)
+            for (int a = 0; a < 3; a++) {
+                lo[a] = fmin(lo[a], part[6 * b + a]);
+                hi[a] = fmax(hi[a], part[6 * b + 3 + a]);
+            }
+        // seed-grid resolution: about one cell per key, power-of-two per axis
+        double ext[3], emax = 0.0;
+        for (int a = 0; a < 3; a++) {
+            ext[a] = hi[a] - lo[a];
+            if (!(ext[a] > 0.0) || !isfinite(ext[a])) ext[a] = 0.0;
+            emax = fmax(emax, ext[a]);
+        }
+        if (!(emax > 0.0)) emax = 1.0;
+        double vol = 1.0;
+        for (int a = 0; a < 3; a++) {
+            if (ext[a] < emax * 1e-3) ext[a] = emax * 1e-3;
+            vol *= ext[a];
+        }
+        const size_t cmax = grid_cells_max(n_vertices);
+        const double side = cbrt(vol / (double)cmax);
+        int R[3], lv[3];
+        for (int a = 0; a < 3; a++) {
+            double r = ext[a] / side;
+            int l = 0;
+            while (l < 10 && (double)(1 << (l + 1)) <= r * 1.4142) l++;
+            lv[a] = l;
+        }
+        while (((size_t)1 << (lv[0] + lv[1] + lv[2])) > cmax) {
+            int a = (lv[0] >= lv[1] && lv[0] >= lv[2]) ? 0 : (lv[1] >= lv[2] ? 1 : 2);
+            lv[a]--;
+        }
+        for (int a = 0; a < 3; a++) {
+            R[a] = 1 << lv[a];
+            V.gdim[a] = R[a];
+            V.glo[a] = lo[a];
+            V.ginv[a] = (double)R[a] / ext[a];
+        }
+        const int levels = lv[0] > lv[1] ? (lv[0] > lv[2] ? lv[0] : lv[2]) : (lv[1] > lv[2] ? lv[1] : lv[2]);
+        int *cur = L.grid_a, *prev = nullptr;
+        int pd[3] = {1, 1, 1};
+        for (int k = 0; k <= levels; k++) {
+            int d[3];
+            for (int a = 0; a < 3; a++) d[a] = (1 << k) < R[a] ? (1 << k) : R[a];
+            const int nc = d[0] * d[1] * d[2];
+            k_seed_level<<<blocks_for(nc, 128), 128, 0, st>>>(V, d[0], d[1], d[2], pd[0], pd[1], pd[2],
+                                                              prev, cur, L.flag);
+            prev = cur;
+            cur = (cur == L.grid_a) ? L.grid_b : L.grid_a;
+            for (int a = 0; a < 3; a++) pd[a] = d[a];
+        }
+        V.grid = prev;
+        if (cudaMemcpyAsync(flag, L.flag, sizeof(flag), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+            cudaStreamSynchronize(st) != cudaSuccess) {
+            rc = NIF_ERR_CUDA;
+            break;
+        }
+        if (flag[0]) rc = NIF_ERR_INTERNAL;
+        if (cudaGetLastError() != cudaSuccess) rc = NIF_ERR_CUDA;
+    } while (0);
+    if (rc != NIF_OK) {
+        delete h;
+        return rc;
+    }
+    *out = h;
+    return NIF_OK;
+}
+
+NIF_EXPORT void nif_dmesh_destroy(nif_dmesh *m) { delete m; }
+
+NIF_EXPORT int nif_dmesh_info(const nif_dmesh *m, int64_t info[8]) {
+    if (!m || !info) return NIF_ERR_ARG;
+    info[0] = m->n_vertices;
+    info[1] = m->n_tets;
+    info[2] = m->view.gdim[0];
+    info[3] = m->view.gdim[1];
+    info[4] = m->view.gdim[2];
+    info[5] = info[6] = info[7] = 0;
+    return NIF_OK;
+}
+
+NIF_EXPORT int nif_query_workspace_bytes(const nif_dmesh *m, int64_t M, int mode, size_t *bytes) {
+    if (!m || !bytes || M < 0 || (mode != NIF_MODE_WEIGHTS && mode != NIF_MODE_INTERP))
+        return NIF_ERR_ARG;
+    Carve c{nullptr, 0, (size_t)-1, true};
+    carve_query(c, M, mode);
+    *bytes = align_up(c.off, 256);
+    return NIF_OK;
+}
+
+NIF_EXPORT int nif_weights_count(const nif_dmesh *m, const void *d_queries, int query_dtype,
+                                 int64_t M, const double centroid[3], void *d_ws, size_t ws_bytes,
+                                 int32_t *d_rowptr, void *stream, nif_summary *summary) {
+    int rc = check_query_args(m, d_queries, query_dtype, M, centroid, d_ws);
+    if (rc != NIF_OK) return rc;
+    if (!d_rowptr) return NIF_ERR_ARG;
+    size_t need = 0;
+    nif_query_workspace_bytes(m, M, NIF_MODE_WEIGHTS, &need);
+    if (ws_bytes < need) return NIF_ERR_WORKSPACE;
+    cudaStream_t st = S(stream);
+    Carve c{reinterpret_cast<unsigned char *>(d_ws), 0, ws_bytes, true};
+    QueryLayout L = carve_query(c, M, NIF_MODE_WEIGHTS);
+    Centroid cen{{centroid[0], centroid[1], centroid[2]}};
+    NIF_CUDA(cudaMemsetAsync(L.sum, 0, sizeof(DevSummary), st));
+    if (M > 0) {
+        StageSink sink{L.cnt, L.src, L.scols, L.svals, M * ROW_CAP, L.arena_cap, L.sum};
+        if (query_dtype == NIF_F64) {
+            run_bucketing(m, static_cast<const double *>(d_queries), M, cen, L, st);
+            run_rows(m, static_cast<const double *>(d_queries), M, cen, L, sink, st);
+        } else {
+            run_bucketing(m, static_cast<const float *>(d_queries), M, cen, L, st);
+            run_rows(m, static_cast<const float *>(d_queries), M, cen, L, sink, st);
+        }
+    }
+    launch_scan<int64_t>(L.cnt, M, L.scan_bsum, L.scan_total, L.off64, st);
+    k_rowptr_guarded<<<blocks_for(M + 1, 256), 256, 0, st>>>(L.off64, M, L.scan_total, d_rowptr);
+    if (M > 0) prof_mark(4, st);
+    int64_t total = 0;
+    nif_summary tmp;
+    rc = read_summary(L, st, summary ? summary : &tmp, &total);
+    if (rc != NIF_OK) return rc;
+    if (total > (int64_t)INT32_MAX) return NIF_ERR_OVERFLOW;
+    return NIF_OK;
+}
+
+NIF_EXPORT int nif_weights_fill(const nif_dmesh *m, int64_t M, const void *d_ws, size_t ws_bytes,
+                                const int32_t *d_rowptr, void *d_vals, int vals_dtype,
+                                int32_t *d_cols, void *stream) {
+    if (!m || M < 0 || M > (int64_t)INT32_MAX || !d_ws || !d_rowptr) return NIF_ERR_ARG;
+    if (vals_dtype != NIF_F64 && vals_dtype != NIF_F32) return NIF_ERR_ARG;
+    size_t need = 0;
+    nif_query_workspace_bytes(m, M, NIF_MODE_WEIGHTS, &need);
+    if (ws_bytes < need) return NIF_ERR_WORKSPACE;
+    if (M == 0) return NIF_OK;
+    if (!d_vals || !d_cols) return NIF_ERR_ARG;
+    cudaStream_t st = S(stream);
+    Carve c{reinterpret_cast<unsigned char *>(const_cast<void *>(d_ws)), 0, ws_bytes, true};
+    QueryLayout L = carve_query(c, M, NIF_MODE_WEIGHTS);
+    const int blocks = blocks_for(M * 16, 256);
+    if (vals_dtype == NIF_F64)
+        k_compact<double><<<blocks, 256, 0, st>>>(M, L.cnt, L.src, L.scols, L.svals, d_rowptr, d_cols,
+                                                  static_cast<double *>(d_vals));
+    else
+        k_compact<float><<<blocks, 256, 0, st>>>(M, L.cnt, L.src, L.scols, L.svals, d_rowptr, d_cols,
+                                                 static_cast<float *>(d_vals));
+    return cuda_rc(cudaGetLastError());
+}
+
+namespace {
+template <class QT, class VT, class CT>
+int interp_typed(const nif_dmesh *m, const void *q, int64_t M, const Centroid &cen, const void *v,
+                 int D, void *out, const QueryLayout &L, cudaStream_t st) {
+    InterpSink<QT, VT, CT> sink{static_cast<const VT *>(v), static_cast<CT *>(out), D};
+    run_bucketing(m, static_cast<const QT *>(q), M, cen, L, st);
+    run_rows(m, static_cast<const QT *>(q), M, cen, L, sink, st);
+    return NIF_OK;
+}
+}  // namespace
+
+NIF_EXPORT int nif_interpolate(const nif_dmesh *m, const void *d_queries, int query_dtype,
+                               int64_t M, const double centroid[3], const void *d_values,
+                               int values_dtype, int D, void *d_out, int out_dtype, void *d_ws,
+                               size_t ws_bytes, void *stream, nif_summary *summary) {
+    int rc = check_query_args(m, d_queries, query_dtype, M, centroid, d_ws);
+    if (rc != NIF_OK) return rc;
+    if (values_dtype != NIF_F64 && values_dtype != NIF_F32) return NIF_ERR_ARG;
+    if (D < 1) return NIF_ERR_ARG;
+    const int expect = (query_dtype == NIF_F32 && values_dtype == NIF_F32) ? NIF_F32 : NIF_F64;
+    if (out_dtype != expect) return NIF_ERR_ARG;
+    if (M > 0 && (!d_values || !d_out)) return NIF_ERR_ARG;
+    size_t need = 0;
+    nif_query_workspace_bytes(m, M, NIF_MODE_INTERP, &need);
+    if (ws_bytes < need) return NIF_ERR_WORKSPACE;
+    cudaStream_t st = S(stream);
+    Carve c{reinterpret_cast<unsigned char *>(d_ws), 0, ws_bytes, true};
+    QueryLayout L = carve_query(c, M, NIF_MODE_INTERP);
+    Centroid cen{{centroid[0], centroid[1], centroid[2]}};
+    NIF_CUDA(cudaMemsetAsync(L.sum, 0, sizeof(DevSummary), st));
+    if (M > 0) {
+        if (query_dtype == NIF_F64 && values_dtype == NIF_F64)
+            rc = interp_typed<double, double, double>(m, d_queries, M, cen, d_values, D, d_out, L, st);
+        else if (query_dtype == NIF_F64)
+            rc = interp_typed<double, float, double>(m, d_queries, M, cen, d_values, D, d_out, L, st);
+        else if (values_dtype == NIF_F32)
+            rc = interp_typed<float, float, float>(m, d_queries, M, cen, d_values, D, d_out, L, st);
+        else
+            rc = interp_typed<float, double, double>(m, d_queries, M, cen, d_values, D, d_out, L, st);
+        if (rc != NIF_OK) return rc;
+    }
+    if (M > 0) prof_mark(4, st);
+    if (summary) return read_summary(L, st, summary, nullptr);
+    return cuda_rc(cudaGetLastError());
+}
+
+NIF_EXPORT int nif_profile_enable(int on) {
+    g_prof.on = on != 0;
+    g_prof.recorded = 0;
+    return NIF_OK;
+}
+
+NIF_EXPORT int nif_profile_read(double ms[4]) {
+    if (!ms) return NIF_ERR_ARG;
+    for (int i = 0; i < 4; i++) ms[i] = 0.0;
+    if (!g_prof.created || g_prof.recorded < PROF_EVENTS) return NIF_ERR_ARG;
+    NIF_CUDA(cudaEventSynchronize(g_prof.ev[PROF_EVENTS - 1]));
+    for (int i = 0; i < 4; i++) {
+        float t = 0.f;
+        NIF_CUDA(cudaEventElapsedTime(&t, g_prof.ev[i], g_prof.ev[i + 1]));
+        ms[i] = t;
+    }
+    return NIF_OK;
+}
+
+NIF_EXPORT int nif_measure_fp64_peak(double *tflops_fused, double *tflops_separate) {
+    if (!tflops_fused || !tflops_separate) return NIF_ERR_ARG;
+    int dev = 0, sms = 0;
+    NIF_CUDA(cudaGetDevice(&dev));
+    NIF_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    double *out = nullptr;
+    NIF_CUDA(cudaMalloc(&out, sizeof(double)));
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    const int blocks = sms * 8, threads = 256, iters = 4096;
+    const double flops = 2.0 * 8.0 * iters * (double)blocks * threads;
+    double best[2] = {0.0, 0.0};
+    for (int rep = 0; rep < 4; rep++) {
+        for (int v = 0; v < 2; v++) {
+            cudaEventRecord(e0);
+            if (v == 0)
+                k_fp64_peak<true><<<blocks, threads>>>(out, iters, 0.999999, 1e-7);
+            else
+                k_fp64_peak<false><<<blocks, threads>>>(out, iters, 0.999999, 1e-7);
+            cudaEventRecord(e1);
+            cudaEventSynchronize(e1);
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            const double tf = flops / (ms * 1e-3) / 1e12;
+            if (rep > 0 && tf > best[v]) best[v] = tf;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(out);
+    *tflops_fused = best[0];
+    *tflops_separate = best[1];
+    return cuda_rc(cudaGetLastError());
+}

@@ -1,0 +1,161 @@
+"""Device-resident mesh and the query calls of libnif_cuda.so.
+
+PyTorch provides device memory and the stream; the computation is the
+library's own sm_100a kernels.  All tensors passed to the library are
+contiguous CUDA tensors on the mesh's device.
+"""
+import ctypes
+
+import numpy as np
+import torch
+
+from . import _native as N
+
+_DT = {torch.float64: N.NIF_F64, torch.float32: N.NIF_F32}
+_NP_DT = {np.dtype(np.float64): N.NIF_F64, np.dtype(np.float32): N.NIF_F32}
+
+
+def _stream_ptr(device):
+    return ctypes.c_void_p(torch.cuda.current_stream(device).cuda_stream)
+
+
+def _vp(t):
+    return ctypes.c_void_p(t.data_ptr()) if t is not None and t.numel() > 0 else ctypes.c_void_p(0)
+
+
+def _check_device_tensor(t, device, name):
+    if not isinstance(t, torch.Tensor) or t.device != device:
+        raise ValueError('%s must be a tensor on %s' % (name, device))
+
+
+class DeviceMesh:
+    """natinterp3d's mesh uploaded to one GPU (resident arrays + seed grid)."""
+
+    def __init__(self, vxyz, tet_v, tet_n, device=None):
+        if not torch.cuda.is_available():
+            raise RuntimeError('natinterp3d_b200 needs a CUDA device (there is no CPU query path)')
+        self.device = torch.device('cuda', torch.cuda.current_device() if device is None
+                                   else torch.device(device).index or 0)
+        self._lib = N.cuda_lib()
+        vxyz = np.ascontiguousarray(vxyz, np.float64)
+        tet_v = np.ascontiguousarray(tet_v, np.int32)
+        tet_n = np.ascontiguousarray(tet_n, np.int32)
+        self.n_vertices, self.n_tets = int(vxyz.shape[0]), int(tet_v.shape[0])
+        self.n_keys = self.n_vertices - 4
+        nbytes = ctypes.c_size_t()
+        N.check(self._lib.nif_dmesh_bytes(self.n_vertices, self.n_tets, ctypes.byref(nbytes)),
+                'nif_dmesh_bytes')
+        with torch.cuda.device(self.device):
+            self._buf = torch.empty(int(nbytes.value), dtype=torch.uint8, device=self.device)
+            d_v = torch.from_numpy(vxyz).to(self.device)
+            d_tv = torch.from_numpy(tet_v).to(self.device)
+            d_tn = torch.from_numpy(tet_n).to(self.device)
+            self._h = ctypes.c_void_p()
+            N.check(self._lib.nif_dmesh_create(_vp(d_v), _vp(d_tv), _vp(d_tn), self.n_vertices,
+                                               self.n_tets, _vp(self._buf), nbytes.value,
+                                               _stream_ptr(self.device), ctypes.byref(self._h)),
+                    'nif_dmesh_create')
+        info = (ctypes.c_int64 * 8)()
+        N.check(self._lib.nif_dmesh_info(self._h, info), 'nif_dmesh_info')
+        self.grid_dims = (info[2], info[3], info[4])
+
+    @property
+    def nbytes(self):
+        return self._buf.numel()
+
+    def workspace_bytes(self, M, mode):
+        nb = ctypes.c_size_t()
+        N.check(self._lib.nif_query_workspace_bytes(self._h, int(M), mode, ctypes.byref(nb)),
+                'nif_query_workspace_bytes')
+        return int(nb.value)
+
+    def _workspace(self, M, mode):
+        return torch.empty(self.workspace_bytes(M, mode), dtype=torch.uint8, device=self.device)
+
+    @staticmethod
+    def _raise_rows(summary):
+        if summary.rows_failed:
+            code = summary.first_status
+            if code == N.NIF_ERR_WALK:
+                raise RuntimeError('%d queries did not converge in the point-location walk '
+                                   '(step limit reached)' % summary.rows_failed)
+            raise RuntimeError('%d queries exceed the per-query capacity of the large-row kernel '
+                               '(cavity larger than 4096 tets)' % summary.rows_failed)
+
+    def weights_csr(self, q, centroid, vals_dtype=torch.float64, return_summary=False):
+        """Sibson weights of device queries q [M, 3] (float32/float64, caller frame).
+
+        Returns (rowptr int32 [M+1], cols int32 [nnz], vals [nnz]) on the device.
+        """
+        _check_device_tensor(q, self.device, 'queries')
+        q = q.contiguous()
+        if q.dim() != 2 or q.shape[1] != 3:
+            raise ValueError('Query points must have shape (num_query_points, 3)')
+        if q.dtype not in _DT:
+            q = q.to(torch.float64)
+        M = int(q.shape[0])
+        cen = (ctypes.c_double * 3)(*[float(c) for c in centroid])
+        with torch.cuda.device(self.device):
+            ws = self._workspace(M, N.NIF_MODE_WEIGHTS)
+            rowptr = torch.empty(M + 1, dtype=torch.int32, device=self.device)
+            summ = N.Summary()
+            rc = self._lib.nif_weights_count(self._h, _vp(q), _DT[q.dtype], M, cen, _vp(ws),
+                                             ws.numel(), _vp(rowptr), _stream_ptr(self.device),
+                                             ctypes.byref(summ))
+            if rc == N.NIF_ERR_OVERFLOW:
+                raise OverflowError('Total number of nonzero weights exceeds int32 limit')
+            N.check(rc, 'nif_weights_count')
+            self._raise_rows(summ)
+            nnz = int(summ.nnz)
+            cols = torch.empty(nnz, dtype=torch.int32, device=self.device)
+            vals = torch.empty(nnz, dtype=vals_dtype, device=self.device)
+            N.check(self._lib.nif_weights_fill(self._h, M, _vp(ws), ws.numel(), _vp(rowptr),
+                                               _vp(vals), _DT[vals_dtype], _vp(cols),
+                                               _stream_ptr(self.device)), 'nif_weights_fill')
+        if return_summary:
+            return rowptr, cols, vals, summ.as_dict()
+        return rowptr, cols, vals
+
+    def interpolate(self, q, values, centroid, return_summary=False, check=True):
+        """out[M, D] = W(q) @ values without materialising W (device tensors)."""
+        _check_device_tensor(q, self.device, 'queries')
+        _check_device_tensor(values, self.device, 'values')
+        q = q.contiguous()
+        if q.dim() != 2 or q.shape[1] != 3:
+            raise ValueError('Query points must have shape (num_query_points, 3)')
+        if values.dim() not in (1, 2) or values.shape[0] != self.n_keys:
+            raise ValueError('values must have shape (%d,) or (%d, D)' % (self.n_keys, self.n_keys))
+        squeeze = values.dim() == 1
+        v = values.reshape(self.n_keys, -1).contiguous()
+        if q.dtype not in _DT or v.dtype not in _DT:
+            raise TypeError('queries and values must be float32 or float64')
+        out_dtype = torch.float32 if (q.dtype == torch.float32 and v.dtype == torch.float32) \
+            else torch.float64
+        M, D = int(q.shape[0]), int(v.shape[1])
+        cen = (ctypes.c_double * 3)(*[float(c) for c in centroid])
+        with torch.cuda.device(self.device):
+            ws = self._workspace(M, N.NIF_MODE_INTERP)
+            out = torch.empty((M, D), dtype=out_dtype, device=self.device)
+            summ = N.Summary()
+            N.check(self._lib.nif_interpolate(self._h, _vp(q), _DT[q.dtype], M, cen, _vp(v),
+                                              _DT[v.dtype], D, _vp(out), _DT[out_dtype], _vp(ws),
+                                              ws.numel(), _stream_ptr(self.device),
+                                              ctypes.byref(summ) if check else None),
+                    'nif_interpolate')
+            if check:
+                self._raise_rows(summ)
+        out = out[:, 0] if squeeze else out
+        if return_summary:
+            return out, summ.as_dict()
+        return out
+
+    def close(self):
+        if getattr(self, '_h', None) is not None and self._h.value:
+            self._lib.nif_dmesh_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

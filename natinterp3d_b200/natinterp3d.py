@@ -1,0 +1,210 @@
+"""natinterp3d's public API (natinterp3d.py:9-137 of natinterp3d), on one GPU.
+
+Same names, arguments, return types and errors:
+
+* ``Interpolator(data_points, parallel=True, num_threads=None)`` builds the
+  Delaunay tetrahedralization with natinterp3d's own constructor, then keeps
+  the mesh resident on the GPU;
+* ``Interpolator.get_weights(query_points)`` -> ``scipy.sparse.csr_matrix``
+  (M, N) with int32 indices, dtype = query dtype, columns of each row in
+  natinterp3d's order;
+* ``Interpolator.interpolate(query_points, values)`` -> ndarray (M,) or (M, D);
+* module-level ``get_weights`` / ``interpolate``.
+
+``parallel`` and ``num_threads`` are accepted for compatibility and have no
+effect.  ``device`` selects the CUDA device (default: the current one).
+There is no CPU fallback: without a CUDA device the query methods raise.
+
+Device-resident variants (``get_weights_device``, ``interpolate_device``)
+take and return torch tensors on the mesh's GPU.
+"""
+import os
+from typing import Optional
+
+import numpy as np
+import scipy.sparse
+import torch
+
+from ._native import HostMesh
+from .device import DeviceMesh
+
+_FLOATS = (np.dtype(np.float32), np.dtype(np.float64))
+
+
+def interpolate(
+    queries: np.ndarray,
+    keys: np.ndarray,
+    values: np.ndarray,
+    parallel: bool = True,
+    num_threads: Optional[int] = None,
+    device=None,
+) -> np.ndarray:
+    """Natural-neighbour (Sibson) interpolation of ``values`` known at ``keys``,
+    evaluated at ``queries``.  Shapes: queries (M, 3), keys (N, 3), values (N,)
+    or (N, D); returns (M,) or (M, D)."""
+    interpolator = Interpolator(keys, parallel=parallel, num_threads=num_threads, device=device)
+    return interpolator.interpolate(queries, values)
+
+
+def get_weights(
+    queries: np.ndarray,
+    keys: np.ndarray,
+    parallel: bool = True,
+    num_threads: Optional[int] = None,
+    device=None,
+) -> scipy.sparse.csr_matrix:
+    """Sibson coordinates of ``queries`` with respect to ``keys`` as an (M, N)
+    CSR matrix."""
+    interpolator = Interpolator(keys, parallel=parallel, num_threads=num_threads, device=device)
+    return interpolator.get_weights(queries)
+
+
+class Interpolator:
+    """Natural-neighbour interpolator for 3-D data points.
+
+    Build once per key set and reuse: the Delaunay construction (natinterp3d's
+    own, on the host) is the expensive part; queries run on the GPU.
+
+    Args:
+        data_points: (N, 3) data sites.
+        parallel, num_threads: accepted for compatibility with natinterp3d; unused.
+        device: CUDA device for the resident mesh (default: current device).
+        keep_host_mesh: keep natinterp3d's host mesh object alive (only needed
+            to run natinterp3d's CPU query on the same mesh for comparison).
+    """
+
+    def __init__(
+        self,
+        data_points: np.ndarray,
+        parallel: bool = True,
+        num_threads: Optional[int] = None,
+        device=None,
+        keep_host_mesh: bool = False,
+    ):
+        data_points = np.ascontiguousarray(data_points, np.float64)
+        if data_points.ndim != 2 or data_points.shape[1] != 3:
+            raise ValueError('Data points must have shape (num_data_points, 3)')
+        # natinterp3d.py:88-90: centre on the key centroid before triangulating
+        self._centroid = data_points.mean(axis=0)
+        centered = data_points - self._centroid
+        self.n_keys = int(data_points.shape[0])
+        self.parallel = parallel
+        self.num_threads = num_threads
+        host = HostMesh(centered)
+        self.degeneracies = host.degeneracies()
+        self.mesh_arrays = host.export()
+        self.host_mesh = host if keep_host_mesh else None
+        if not keep_host_mesh:
+            host.close()
+        self._device_arg = device
+        self._dmesh = None
+
+    @classmethod
+    def from_mesh(cls, centroid, vxyz, tet_v, tet_n, device=None):
+        """An interpolator over an already exported mesh (see :meth:`save_mesh`)."""
+        self = cls.__new__(cls)
+        self._centroid = np.asarray(centroid, np.float64).reshape(3)
+        self.mesh_arrays = (np.ascontiguousarray(vxyz, np.float64),
+                            np.ascontiguousarray(tet_v, np.int32),
+                            np.ascontiguousarray(tet_n, np.int32))
+        self.n_keys = self.mesh_arrays[0].shape[0] - 4
+        self.parallel, self.num_threads = True, None
+        self.degeneracies = None
+        self.host_mesh = None
+        self._device_arg = device
+        self._dmesh = None
+        return self
+
+    def save_mesh(self, path):
+        """Write the centroid and the packed mesh to an .npz file."""
+        vxyz, tet_v, tet_n = self.mesh_arrays
+        np.savez(path, centroid=self._centroid, vxyz=vxyz, tet_v=tet_v, tet_n=tet_n)
+
+    @classmethod
+    def load_mesh(cls, path, device=None):
+        z = np.load(path)
+        return cls.from_mesh(z['centroid'], z['vxyz'], z['tet_v'], z['tet_n'], device=device)
+
+    @property
+    def centroid(self):
+        return self._centroid
+
+    @property
+    def device_mesh(self) -> DeviceMesh:
+        if self._dmesh is None:
+            self._dmesh = DeviceMesh(*self.mesh_arrays, device=self._device_arg)
+        return self._dmesh
+
+    @property
+    def device(self):
+        return self.device_mesh.device
+
+    # ------------------------------------------------------------------ host API
+    def get_weights(self, query_points: np.ndarray) -> scipy.sparse.csr_matrix:
+        """Natural interpolation weights (Sibson coordinates) of the query points."""
+        query_points = np.asarray(query_points)
+        out_dtype = query_points.dtype
+        q = self._host_queries(query_points)
+        dm = self.device_mesh
+        qd = torch.from_numpy(q).to(dm.device)
+        vals_dtype = torch.float32 if out_dtype == np.float32 else torch.float64
+        rowptr, cols, vals = dm.weights_csr(qd, self._centroid, vals_dtype=vals_dtype)
+        M = q.shape[0]
+        W = scipy.sparse.csr_matrix(
+            (vals.cpu().numpy(), cols.cpu().numpy(), rowptr.cpu().numpy()),
+            shape=(M, self.n_keys))
+        return W.astype(out_dtype, copy=False)
+
+    def interpolate(self, query_points: np.ndarray, values: np.ndarray) -> np.ndarray:
+        """Interpolated values at the query points: (M,) for values (N,), (M, D)
+        for values (N, D)."""
+        query_points = np.asarray(query_points)
+        values = np.asarray(values)
+        qdt = query_points.dtype
+        if qdt not in _FLOATS or values.dtype not in _FLOATS or values.ndim not in (1, 2):
+            # dtypes the fused kernel does not cover: the weights still come
+            # from the GPU and scipy forms the product, as natinterp3d does
+            weights = self.get_weights(query_points)
+            if len(values.shape) == 1:
+                return np.squeeze(weights @ values[:, np.newaxis], axis=1)
+            return weights @ values
+        if values.shape[0] != self.n_keys:
+            raise ValueError('dimension mismatch')
+        q = self._host_queries(query_points)
+        dm = self.device_mesh
+        qd = torch.from_numpy(q).to(dm.device)
+        vd = torch.from_numpy(np.ascontiguousarray(values)).to(dm.device)
+        out = dm.interpolate(qd, vd, self._centroid)
+        return out.cpu().numpy()
+
+    # -------------------------------------------------------- device-resident API
+    def get_weights_device(self, queries: torch.Tensor, dtype=None, as_torch_csr=False):
+        """Weights of device queries; returns (rowptr, cols, vals) device tensors
+        or a ``torch.sparse_csr_tensor`` when ``as_torch_csr``."""
+        dm = self.device_mesh
+        vdt = dtype or (torch.float32 if queries.dtype == torch.float32 else torch.float64)
+        rowptr, cols, vals = dm.weights_csr(queries, self._centroid, vals_dtype=vdt)
+        if as_torch_csr:
+            return torch.sparse_csr_tensor(rowptr, cols, vals, size=(queries.shape[0], self.n_keys))
+        return rowptr, cols, vals
+
+    def interpolate_device(self, queries: torch.Tensor, values: torch.Tensor, check=True):
+        return self.device_mesh.interpolate(queries, values, self._centroid, check=check)
+
+    # ------------------------------------------------------------------ helpers
+    @staticmethod
+    def _host_queries(query_points):
+        if query_points.ndim != 2 or query_points.shape[1] != 3:
+            raise ValueError('Query points must have shape (num_query_points, 3)')
+        if query_points.dtype in _FLOATS:
+            # the device converts float32 to float64 exactly, then subtracts
+            # the centroid in float64 (natinterp3d.py:115)
+            return np.ascontiguousarray(query_points)
+        return np.ascontiguousarray(query_points, np.float64)
+
+
+def default_num_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
