@@ -34,13 +34,19 @@ namespace nif {
 // ---------------------------------------------------------------------------
 // capacities
 // ---------------------------------------------------------------------------
-constexpr int FAST_G = 32;
-using FastWS = Workspace<256, 96, 128, 64, 128, 384, FAST_G>;
+#ifndef NIF_FAST_G
+#define NIF_FAST_G 32
+#endif
+#ifndef NIF_FAST_MINB
+#define NIF_FAST_MINB 6
+#endif
+constexpr int FAST_G = NIF_FAST_G;    // lanes per query in the shared-memory kernel
+using FastWS = Workspace<256, 96, 128, 64, 128, FAST_G, uint8_t, int8_t>;
 constexpr int LARGE_G = 32;
-using LargeWS = Workspace<16384, 4096, 8192, 2048, 8192, 40960, LARGE_G>;
+using LargeWS = Workspace<16384, 4096, 8192, 2048, 8192, LARGE_G, uint16_t, int16_t>;
 constexpr int ROW_CAP = FastWS::NBR;  // staged entries per row
 
-constexpr int FAST_BLOCK = 128;       // 4 groups of 32 lanes
+constexpr int FAST_BLOCK = 128;       // 4 warps
 constexpr int LARGE_GROUPS = 64;      // concurrent large-row groups (one warp each)
 constexpr int SCAN_TILE = 2048;
 constexpr int SCAN_THREADS = 256;
@@ -361,7 +367,7 @@ struct StageSink {
         }
         for (int s = g.lane; s < nnb; s += G) {
             cols[o + s] = ws.nbr_vid[s];
-            vals[o + s] = ws.w[s];
+            vals[o + s] = ws.acc[s];
         }
         if (g.lane == 0) {
             cnt[i] = nnb;
@@ -387,12 +393,16 @@ template <> struct Arith<float> {
 };
 
 // interpolate: out[i, :] = sum over the row of (CT)(WT)w * (CT)values[col, :],
-// accumulated in stored order from zero (scipy csr_matvec / csr_matvecs)
+// accumulated from zero in stored order (scipy csr_matvec / csr_matvecs).
+// natinterp3d's get_weights ends with W.astype(query dtype); for a float32
+// query that conversion also canonicalises the CSR (columns sorted within each
+// row), so with WT = float the row is accumulated in ascending column order.
 template <class WT, class VT, class CT>
 struct InterpSink {
     const VT *__restrict__ values;  // [N][D]
     CT *__restrict__ out;           // [M][D]
     int D;
+    static constexpr bool SORTED = sizeof(WT) == 4;
 
     template <int G, class W>
     __device__ __forceinline__ void emit(int64_t i, int nnb, W &ws, const Grp<G> &g, bool) {
@@ -401,17 +411,28 @@ struct InterpSink {
             for (int d = g.lane; d < D; d += G) o[d] = (CT)0;
             return;
         }
-        // products staged in the (now free) term buffer, dc columns at a time
-        double *buf = ws.u.b.terms;
-        const int dc = max(1, min(D, W::TERMS / nnb));
+        // the cavity-search scratch is free now: stage the products there
+        double *buf = reinterpret_cast<double *>(&ws.u);
+        constexpr int BUFN = (int)(sizeof(ws.u) / sizeof(double));
+        if (SORTED) {
+            // position of each neighbour in ascending column order (columns are distinct)
+            for (int s = g.lane; s < nnb; s += G) {
+                const int v = ws.nbr_vid[s];
+                int r = 0;
+                for (int t = 0; t < nnb; t++) r += ws.nbr_vid[t] < v;
+                ws.vh_first[s] = r;
+            }
+        }
+        const int dc = max(1, min(D, BUFN / nnb));
         for (int d0 = 0; d0 < D; d0 += dc) {
             const int nd = min(dc, D - d0);
             g.sync();
             for (int k = g.lane; k < nnb * nd; k += G) {
                 const int s = k / nd, d = k - s * nd;
-                const CT w = (CT)(WT)ws.w[s];
+                const CT w = (CT)(WT)ws.acc[s];
                 const CT x = (CT)values[(int64_t)ws.nbr_vid[s] * D + d0 + d];
-                buf[k] = (double)Arith<CT>::mul(w, x);
+                const int row = SORTED ? ws.vh_first[s] : s;
+                buf[row * nd + d] = (double)Arith<CT>::mul(w, x);
             }
             g.sync();
             for (int d = g.lane; d < nd; d += G) {
@@ -444,7 +465,7 @@ __device__ __forceinline__ void record(DevSummary *sum, const RowInfo &r, int la
 
 // fast path: shared-memory scratch, rows in bucket order
 template <class QT, class Sink>
-__global__ void __launch_bounds__(FAST_BLOCK) k_rows_fast(MeshView M, const QT *__restrict__ Q,
+__global__ void __launch_bounds__(FAST_BLOCK, NIF_FAST_MINB) k_rows_fast(MeshView M, const QT *__restrict__ Q,
                                                           Centroid cen, const int *__restrict__ order,
                                                           int64_t nrows, Sink sink, LargeQueue lq,
                                                           DevSummary *sum) {
@@ -695,24 +716,6 @@ void launch_scan(const int *in, int64_t n, OutT *bsum, OutT *total, OutT *out, c
     k_scan_apply<OutT><<<(unsigned)nb, SCAN_THREADS, 0, st>>>(in, n, bsum, out);
 }
 
-int fast_grid(const nif_dmesh *m, int64_t M) {
-    static int per_sm = -1;
-    if (per_sm < 0) {
-        per_sm = 0;
-        // occupancy is identical for every instantiation (same block and smem)
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-            &per_sm, k_rows_fast<double, StageSink>, FAST_BLOCK,
-            (FAST_BLOCK / FAST_G) * sizeof(FastWS));
-        if (per_sm < 1) per_sm = 1;
-    }
-    const int64_t groups = (M + 0) / 1;
-    int64_t blocks = (groups + (FAST_BLOCK / FAST_G) - 1) / (FAST_BLOCK / FAST_G);
-    const int64_t cap = (int64_t)per_sm * m->num_sms;
-    if (blocks > cap) blocks = cap;
-    if (blocks < 1) blocks = 1;
-    return (int)blocks;
-}
-
 template <class Kern>
 int set_smem(Kern k, size_t bytes) {
     return cuda_rc(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
@@ -759,9 +762,22 @@ void run_bucketing(const nif_dmesh *m, const QT *Q, int64_t M, const Centroid &c
 template <class QT, class Sink>
 void run_rows(const nif_dmesh *m, const QT *Q, int64_t M, const Centroid &cen, const QueryLayout &L,
               const Sink &sink, cudaStream_t st) {
-    const size_t smem = (FAST_BLOCK / FAST_G) * sizeof(FastWS);
-    k_rows_fast<QT, Sink><<<fast_grid(m, M), FAST_BLOCK, smem, st>>>(
-        m->view, Q, cen, L.order, M, sink, LargeQueue{L.large_list}, L.sum);
+    constexpr int GPB = FAST_BLOCK / FAST_G;
+    const size_t smem = GPB * sizeof(FastWS);
+    auto kern = k_rows_fast<QT, Sink>;
+    static int per_sm = -1;  // resident blocks per SM of this instantiation
+    if (per_sm < 0) {
+        if (smem > 48 * 1024) set_smem(kern, smem);
+        per_sm = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, FAST_BLOCK, smem);
+        if (per_sm < 1) per_sm = 1;
+    }
+    int64_t blocks = (M + GPB - 1) / GPB;
+    const int64_t cap = (int64_t)per_sm * m->num_sms;
+    if (blocks > cap) blocks = cap;
+    if (blocks < 1) blocks = 1;
+    kern<<<(unsigned)blocks, FAST_BLOCK, smem, st>>>(m->view, Q, cen, L.order, M, sink,
+                                                    LargeQueue{L.large_list}, L.sum);
     prof_mark(2, st);
     k_rows_large<QT, Sink><<<LARGE_GROUPS, 32, 0, st>>>(m->view, Q, cen, LargeQueue{L.large_list},
                                                         sink, L.large_ws, L.sum);

@@ -12,8 +12,8 @@
 //               floating-point summation order of every weight
 //   3. boundary faces and natural neighbours in first-seen order (:559-584)
 //   4. signed Voronoi-subcell volumes: +cavity-tet terms (:642-676) and
-//      -virtual-tet terms (:681-719), one term per lane, written to a
-//      slot-sorted buffer and summed per neighbour in natinterp3d's order
+//      -virtual-tet terms (:681-719), one term per lane, folded into each
+//      neighbour's sum in natinterp3d's accumulation order
 //   5. normalisation (:721-737)
 // Tet circumcentres and face circumcentres are read from the per-mesh cache
 // (computed with the same formulas and argument orders); a face shared by two
@@ -70,6 +70,10 @@ __device__ __forceinline__ dv3 vload(const MeshView &M, int vid) {
     return dv3{v.x, v.y, v.z};
 }
 
+__device__ __forceinline__ void prefetch_l2(const void *p) {
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+}
+
 __device__ __forceinline__ dv3 cload(const d4 *p) {
     const d4 v = *p;
     return dv3{v.x, v.y, v.z};
@@ -114,9 +118,9 @@ struct Grp {
 };
 
 // Per-group scratch.  The first union member is live during the cavity
-// search, the second only during the single-lane replay, the third during
-// the volume terms and the interpolation epilogue.
-template <int HS_, int CAV_, int BF_, int NBR_, int VH_, int TERMS_, int G_>
+// search, the second only during the single-lane replay of natinterp3d's
+// visiting order.  Index types are the narrowest that hold each capacity.
+template <int HS_, int CAV_, int BF_, int NBR_, int VH_, int G_, class SlotT, class CavT>
 struct Workspace {
     static constexpr int HS = HS_;        // tested-tet hash slots (power of two)
     static constexpr int QCAP = HS_ * 3 / 4;
@@ -125,35 +129,29 @@ struct Workspace {
     static constexpr int BF = BF_;        // boundary faces
     static constexpr int NBR = NBR_;      // natural neighbours
     static constexpr int VH = VH_;        // neighbour hash slots (power of two)
-    static constexpr int TERMS = TERMS_;  // volume terms
     static constexpr int G = G_;
+    using slot_t = SlotT;                 // tested-tet hash slot index
+    using cav_t = CavT;                   // signed cavity index
     union U {
         struct {
             int hkey[HS_];
-            int hval[HS_];
-            int queue[HS_ * 3 / 4];
+            CavT hval[HS_];
+            SlotT queue[HS_ * 3 / 4];
         } a;
         struct {
-            int stack[4 * CAV_ + 1];
+            CavT stack[4 * CAV_ + 1];
         } r;
-        struct {
-            double terms[TERMS_];
-            double vt[G_][3];
-        } b;
     } u;
+    double acc[NBR_];            // stolen volume per neighbour
     int cav_tet[CAV_];
-    int cav_nbr[4 * CAV_];
-    int order[CAV_];
-    int pos[CAV_];
-    int bface[BF_];
+    int nbr_vid[NBR_];
     int vh_key[VH_];
     int vh_first[VH_];
-    int vh_slot[VH_];
-    int nbr_vid[NBR_];
-    int cnt[NBR_];
-    int off[NBR_];
-    int run[NBR_];
-    double w[NBR_];
+    CavT cav_nbr[4 * CAV_];      // cavity index of neighbour f of cavity tet c, -1 outside
+    CavT order[CAV_];            // cavity tets in natinterp3d's visiting order
+    CavT pos[CAV_];              // inverse of order
+    uint16_t bface[BF_];         // (cavity index << 2) | face
+    int16_t vh_slot[VH_];
 };
 
 __device__ __forceinline__ unsigned mix_hash(int key) {
@@ -164,6 +162,7 @@ __device__ __forceinline__ unsigned mix_hash(int key) {
 // Sets full when every slot was probed.
 __device__ __forceinline__ int hash_insert(int *keys, int hs, int key, bool &full) {
     unsigned h = mix_hash(key) & (unsigned)(hs - 1);
+#pragma unroll 1
     for (int probe = 0; probe < hs; ++probe) {
         const int old = atomicCAS(&keys[h], -1, key);
         if (old == -1) return (int)h;
@@ -177,6 +176,7 @@ __device__ __forceinline__ int hash_insert(int *keys, int hs, int key, bool &ful
 // Slot of key (inserted if absent); -1 and full=true when the table is full.
 __device__ __forceinline__ int hash_upsert(int *keys, int hs, int key, bool &full) {
     unsigned h = mix_hash(key) & (unsigned)(hs - 1);
+#pragma unroll 1
     for (int probe = 0; probe < hs; ++probe) {
         const int old = atomicCAS(&keys[h], -1, key);
         if (old == -1 || old == key) return (int)h;
@@ -188,6 +188,7 @@ __device__ __forceinline__ int hash_upsert(int *keys, int hs, int key, bool &ful
 
 __device__ __forceinline__ int hash_find(const int *keys, int hs, int key) {
     unsigned h = mix_hash(key) & (unsigned)(hs - 1);
+#pragma unroll 1
     for (int probe = 0; probe < hs; ++probe) {
         const int k = keys[h];
         if (k == key) return (int)h;
@@ -227,9 +228,11 @@ __device__ __forceinline__ int neighbour_slot(const W &ws, int v) {
 }
 
 // The Sibson row of centred query q.  On ST_OK the row is ws.nbr_vid[0..nnb)
-// with normalised weights ws.w[0..nnb), in natinterp3d's column order.
+// with normalised weights ws.acc[0..nnb), in natinterp3d's column order.
 template <int G, class W>
 __device__ RowInfo sibson_row(const MeshView &M, const dv3 q, W &ws, const Grp<G> &g) {
+    using cav_t = typename W::cav_t;
+    using slot_t = typename W::slot_t;
     RowInfo r{ST_OK, 0, 0, false};
 
     // ---- 1. point location -------------------------------------------------
@@ -263,13 +266,13 @@ __device__ RowInfo sibson_row(const MeshView &M, const dv3 q, W &ws, const Grp<G
     // ---- 2. cavity: parallel flood over the tested-tet hash ----------------
     for (int i = g.lane; i < W::HS; i += G) {
         ws.u.a.hkey[i] = -1;
-        ws.u.a.hval[i] = -1;
+        ws.u.a.hval[i] = (cav_t)-1;
     }
     g.sync();
     if (g.lane == 0) {
         const int h = (int)(mix_hash(start) & (unsigned)(W::HS - 1));
         ws.u.a.hkey[h] = start;
-        ws.u.a.queue[0] = h;
+        ws.u.a.queue[0] = (slot_t)h;
     }
     g.sync();
     int qhead = 0, qtail = 1, ncav = 0;
@@ -283,14 +286,20 @@ __device__ RowInfo sibson_row(const MeshView &M, const dv3 q, W &ws, const Grp<G
             tt = ws.u.a.hkey[slot];
             const int4 p = M.tv[tt];
             const dv3 a = vload(M, p.x), b = vload(M, p.y), c = vload(M, p.z), d = vload(M, p.w);
-            const double ins = (M.tinfo[tt] & 1u) ? insphere_fast(a, b, c, d, q)
-                                                  : insphere_fast(b, a, c, d, q);
-            inc = ins > 0;
+            // insphere argument order fixed by the tet's orientation
+            // (natural_insertionfree.c:511-515)
+            const bool pos = (M.tinfo[tt] & 1u) != 0;
+            inc = insphere_fast(pos ? a : b, pos ? b : a, c, d, q) > 0;
         }
         const unsigned cm = g.ballot(inc);
         const int ci = ncav + __popc(cm & g.lt());
-        if (g.lane < n) ws.u.a.hval[slot] = inc ? ci : -1;
-        if (inc && ci < W::CAV) ws.cav_tet[ci] = tt;
+        if (g.lane < n) ws.u.a.hval[slot] = (cav_t)(inc ? ci : -1);
+        if (inc && ci < W::CAV) {
+            ws.cav_tet[ci] = tt;
+            // the volume phase reads this tet's cached circumcentres
+            prefetch_l2(&M.tcc[tt]);
+            prefetch_l2(&M.fcc[4 * (size_t)tt]);
+        }
         const int nnew = __popc(cm);
         const int base = ncav;
         ncav += nnew;
@@ -310,7 +319,7 @@ __device__ RowInfo sibson_row(const MeshView &M, const dv3 q, W &ws, const Grp<G
             }
             const unsigned pm = g.ballot(ns >= 0);
             const int qi = qtail + __popc(pm & g.lt());
-            if (ns >= 0 && qi < W::QCAP) ws.u.a.queue[qi] = ns;
+            if (ns >= 0 && qi < W::QCAP) ws.u.a.queue[qi] = (slot_t)ns;
             qtail += __popc(pm);
             if (g.any(full) || qtail > W::QCAP) overflow = true;
         }
@@ -334,13 +343,10 @@ __device__ RowInfo sibson_row(const MeshView &M, const dv3 q, W &ws, const Grp<G
         }
         const unsigned cm = g.ballot(co);
         const int nco = __popc(cm);
-        if (nco > 0) {
-            const double w = fdiv(1.0, (double)nco);
-            if (co) {
-                const int s = __popc(cm & g.lt());
-                ws.nbr_vid[s] = v;
-                ws.w[s] = w;
-            }
+        if (co) {
+            const int s = __popc(cm & g.lt());
+            ws.nbr_vid[s] = v;
+            ws.acc[s] = fdiv(1.0, (double)nco);
         }
         g.sync();
         r.nnb = nco;
@@ -353,27 +359,48 @@ __device__ RowInfo sibson_row(const MeshView &M, const dv3 q, W &ws, const Grp<G
         int v = -1;
         if (nb >= 0) {
             const int s = hash_find(ws.u.a.hkey, W::HS, nb);
-            v = (s >= 0) ? ws.u.a.hval[s] : -1;
+            v = (s >= 0) ? (int)ws.u.a.hval[s] : -1;
         }
-        ws.cav_nbr[k] = v;
+        ws.cav_nbr[k] = (cav_t)v;
     }
-    for (int c = g.lane; c < ncav; c += G) ws.pos[c] = -1;
+    for (int c = g.lane; c < ncav; c += G) ws.pos[c] = (cav_t)-1;
     g.sync();
 
     // replay natinterp3d's LIFO flood on the cavity (its non-cavity tets are
     // leaves and do not change the order in which cavity tets are reached)
     if (g.lane == 0) {
-        int *stack = ws.u.r.stack;
+        cav_t *stack = ws.u.r.stack;
         int sp = 0, nord = 0;
         stack[sp++] = 0;
-        while (sp > 0) {
-            const int c = stack[--sp];
-            if (ws.pos[c] >= 0) continue;
-            ws.pos[c] = nord;
-            ws.order[nord++] = c;
-            for (int f = 0; f < 4; f++) {
-                const int nc = ws.cav_nbr[4 * c + f];
-                if (nc >= 0 && ws.pos[nc] < 0) stack[sp++] = nc;
+        if constexpr (W::CAV <= 128) {
+            // visited set in two 64-bit registers
+            uint64_t v0 = 0, v1 = 0;
+            while (sp > 0) {
+                const int c = stack[--sp];
+                const uint64_t bit = 1ull << (c & 63);
+                if ((c < 64 ? v0 : v1) & bit) continue;
+                if (c < 64) v0 |= bit; else v1 |= bit;
+                const int n0 = ws.cav_nbr[4 * c], n1 = ws.cav_nbr[4 * c + 1];
+                const int n2 = ws.cav_nbr[4 * c + 2], n3 = ws.cav_nbr[4 * c + 3];
+                ws.pos[c] = (cav_t)nord;
+                ws.order[nord++] = (cav_t)c;
+                const int nb[4] = {n0, n1, n2, n3};
+#pragma unroll
+                for (int f = 0; f < 4; f++) {
+                    const int nc = nb[f];
+                    if (nc >= 0 && !(((nc < 64 ? v0 : v1) >> (nc & 63)) & 1ull)) stack[sp++] = (cav_t)nc;
+                }
+            }
+        } else {
+            while (sp > 0) {
+                const int c = stack[--sp];
+                if (ws.pos[c] >= 0) continue;
+                ws.pos[c] = (cav_t)nord;
+                ws.order[nord++] = (cav_t)c;
+                for (int f = 0; f < 4; f++) {
+                    const int nc = ws.cav_nbr[4 * c + f];
+                    if (nc >= 0 && ws.pos[nc] < 0) stack[sp++] = (cav_t)nc;
+                }
             }
         }
     }
@@ -391,7 +418,7 @@ __device__ RowInfo sibson_row(const MeshView &M, const dv3 q, W &ws, const Grp<G
         }
         const unsigned bm = g.ballot(isb);
         const int b = nbf + __popc(bm & g.lt());
-        if (isb && b < W::BF) ws.bface[b] = (c << 2) | (k & 3);
+        if (isb && b < W::BF) ws.bface[b] = (uint16_t)((c << 2) | (k & 3));
         nbf += __popc(bm);
     }
     if (nbf > W::BF) {
@@ -437,8 +464,11 @@ __device__ RowInfo sibson_row(const MeshView &M, const dv3 q, W &ws, const Grp<G
         const unsigned fm = g.ballot(first);
         const int slot = nnb + __popc(fm & g.lt());
         if (first) {
-            ws.vh_slot[s] = slot;
-            if (slot < W::NBR) ws.nbr_vid[slot] = v;
+            ws.vh_slot[s] = (int16_t)slot;
+            if (slot < W::NBR) {
+                ws.nbr_vid[slot] = v;
+                ws.acc[slot] = 0.0;
+            }
         }
         nnb += __popc(fm);
     }
@@ -449,158 +479,98 @@ __device__ RowInfo sibson_row(const MeshView &M, const dv3 q, W &ws, const Grp<G
     g.sync();
     if (nnb == 0) return r;
 
-    // ---- 4. volume terms: counting pass --------------------------------------
-    for (int s = g.lane; s < nnb; s += G) ws.cnt[s] = 0;
-    g.sync();
-    for (int k0 = 0; k0 < 4 * ncav; k0 += G) {
+    // ---- 4. stolen volumes ----------------------------------------------------
+    // Items in natinterp3d's order: the 4 vertices of every cavity tet (cavity
+    // order), then the 3 vertices of every boundary face (face order).  Each
+    // lane computes one item's signed subcell volume; lanes whose items belong
+    // to the same neighbour are folded into acc[] by the lowest of them, in
+    // lane order, so every acc[] is a left-to-right sum in item order.
+    const int n_old = 4 * ncav;
+    const int n_all = n_old + 3 * nbf;
+    for (int k0 = 0; k0 < n_all; k0 += G) {
         const int k = k0 + g.lane;
         int s = -1;
-        if (k < 4 * ncav) {
-            const int v = comp(M.tv[ws.cav_tet[ws.order[k >> 2]]], k & 3);
-            if (v < M.n) s = neighbour_slot(ws, v);
-        }
-        const unsigned peers = g.match(s);
-        if (s >= 0 && (__ffs(peers) - 1) == g.lane) ws.cnt[s] += __popc(peers);
-        g.sync();
-    }
-    for (int k0 = 0; k0 < 3 * nbf; k0 += G) {
-        const int k = k0 + g.lane;
-        int s = -1;
-        if (k < 3 * nbf) {
-            const int b = k / 3, j = k - 3 * b;
-            const int cf = ws.bface[b];
-            const int v = comp(M.tv[ws.cav_tet[cf >> 2]], face_vslot(cf & 3, j));
-            if (v < M.n) s = neighbour_slot(ws, v);
-        }
-        const unsigned peers = g.match(s);
-        if (s >= 0 && (__ffs(peers) - 1) == g.lane) ws.cnt[s] += __popc(peers);
-        g.sync();
-    }
-    int nterm = 0;
-    if (g.lane == 0) {
-        for (int s = 0; s < nnb; s++) {
-            ws.off[s] = nterm;
-            ws.run[s] = 0;
-            nterm += ws.cnt[s];
-        }
-    }
-    nterm = g.shfl(nterm, 0);
-    g.sync();
-    if (nterm > W::TERMS) {
-        r.status = ST_CAPACITY;
-        return r;
-    }
-
-    // ---- 4b. volume terms: compute pass (same item order) -------------------
-    // cavity tets: +volume of the subcell of each neighbour vertex
-    for (int k0 = 0; k0 < 4 * ncav; k0 += G) {
-        const int k = k0 + g.lane;
-        int s = -1, c = 0, tt = 0, vi = 0;
-        int4 p = make_int4(0, 0, 0, 0);
-        if (k < 4 * ncav) {
-            c = ws.order[k >> 2];
-            vi = k & 3;
-            tt = ws.cav_tet[c];
-            p = M.tv[tt];
-            const int v = comp(p, vi);
-            if (v < M.n) s = neighbour_slot(ws, v);
-        }
-        const unsigned peers = g.match(s);
-        int dest = 0;
-        if (s >= 0) dest = ws.off[s] + ws.run[s] + __popc(peers & g.lt());
-        g.sync();
-        if (s >= 0 && (__ffs(peers) - 1) == g.lane) ws.run[s] += __popc(peers);
-        if (s >= 0) {
-            const uint32_t info = M.tinfo[tt];
-            // the other three vertices in ascending slot order
-            const int o0 = (vi == 0) ? 1 : 0;
-            const int o1 = (vi <= 1) ? 2 : 1;
-            const int o2 = (vi <= 2) ? 3 : 2;
-            const dv3 pk = vload(M, comp(p, vi));
-            const dv3 pa = vload(M, comp(p, o0));
-            const dv3 pb = vload(M, comp(p, o1));
-            const dv3 pc = vload(M, comp(p, o2));
-            const dv3 ct = cload(&M.tcc[tt]);
-            const dv3 f2 = face_cc(M, ws, c, tt, info, o2);
-            const dv3 f1 = face_cc(M, ws, c, tt, info, o1);
-            const dv3 f0 = face_cc(M, ws, c, tt, info, o0);
-            ws.u.b.terms[dest] = subcell_volume(pk, pa, pb, pc, ct, f2, f1, f0);
-        }
-        g.sync();
-    }
-    // virtual tets (query + boundary face): -volume, faces in chunks of G
-    for (int b0 = 0; b0 < nbf; b0 += G) {
-        {
-            const int b = b0 + g.lane;
-            if (b < nbf) {
+        double term = 0.0;
+        if (k < n_all) {
+            dv3 pk, pa, pb, pc, ct, f1, f2, f3;
+            bool old_term = k < n_old;
+            if (old_term) {
+                // cavity tet c, vertex vi (natural_insertionfree.c:642-676)
+                const int c = ws.order[k >> 2];
+                const int vi = k & 3;
+                const int tt = ws.cav_tet[c];
+                const int4 p = M.tv[tt];
+                const int v = comp(p, vi);
+                if (v < M.n) s = neighbour_slot(ws, v);
+                if (s >= 0) {
+                    const uint32_t info = M.tinfo[tt];
+                    // the other three vertices in ascending slot order
+                    const int o0 = (vi == 0) ? 1 : 0;
+                    const int o1 = (vi <= 1) ? 2 : 1;
+                    const int o2 = (vi <= 2) ? 3 : 2;
+                    pk = vload(M, v);
+                    pa = vload(M, comp(p, o0));
+                    pb = vload(M, comp(p, o1));
+                    pc = vload(M, comp(p, o2));
+                    ct = cload(&M.tcc[tt]);
+                    f1 = face_cc(M, ws, c, tt, info, o2);
+                    f2 = face_cc(M, ws, c, tt, info, o1);
+                    f3 = face_cc(M, ws, c, tt, info, o0);
+                }
+            } else {
+                // virtual tet (query + boundary face), vertex j (:681-719)
+                const int kk = k - n_old;
+                const int b = kk / 3, j = kk - 3 * b;
                 const int cf = ws.bface[b];
                 const int f = cf & 3;
-                const int4 p = M.tv[ws.cav_tet[cf >> 2]];
-                const dv3 fa = vload(M, comp(p, face_vslot(f, 0)));
-                const dv3 fb = vload(M, comp(p, face_vslot(f, 1)));
-                const dv3 fc = vload(M, comp(p, face_vslot(f, 2)));
-                const dv3 cv = tet_cc(q, fa, fb, fc);
-                ws.u.b.vt[g.lane][0] = cv.x;
-                ws.u.b.vt[g.lane][1] = cv.y;
-                ws.u.b.vt[g.lane][2] = cv.z;
-            }
-        }
-        g.sync();
-        const int kend = 3 * min(nbf, b0 + G);
-        for (int k0 = 3 * b0; k0 < kend; k0 += G) {
-            const int k = k0 + g.lane;
-            int s = -1, b = 0, j = 0, tt = 0, f = 0;
-            int4 p = make_int4(0, 0, 0, 0);
-            if (k < kend) {
-                b = k / 3;
-                j = k - 3 * b;
-                const int cf = ws.bface[b];
-                f = cf & 3;
-                tt = ws.cav_tet[cf >> 2];
-                p = M.tv[tt];
-                const int v = comp(p, face_vslot(f, j));
+                const int tt = ws.cav_tet[cf >> 2];
+                const int4 p = M.tv[tt];
+                const int va = comp(p, face_vslot(f, 0));
+                const int vb = comp(p, face_vslot(f, 1));
+                const int vc = comp(p, face_vslot(f, 2));
+                const int v = (j == 0) ? va : (j == 1 ? vb : vc);
                 if (v < M.n) s = neighbour_slot(ws, v);
+                if (s >= 0) {
+                    const dv3 fa = vload(M, va), fb = vload(M, vb), fc = vload(M, vc);
+                    pk = (j == 0) ? fa : (j == 1 ? fb : fc);
+                    pa = q;
+                    pb = (j == 0) ? fb : (j == 1 ? fc : fa);  // face_verts[(j+1)%3]
+                    pc = (j == 0) ? fc : (j == 1 ? fa : fb);  // face_verts[(j+2)%3]
+                    ct = tet_cc(q, fa, fb, fc);
+                    f1 = tri_cc(pk, q, pb);
+                    f2 = tri_cc(pk, q, pc);
+                    f3 = cload(&M.fcc[4 * (size_t)tt + (3 - f)]);
+                }
             }
-            const unsigned peers = g.match(s);
-            int dest = 0;
-            if (s >= 0) dest = ws.off[s] + ws.run[s] + __popc(peers & g.lt());
-            g.sync();
-            if (s >= 0 && (__ffs(peers) - 1) == g.lane) ws.run[s] += __popc(peers);
             if (s >= 0) {
-                const int ja = (j == 2) ? 0 : j + 1;
-                const int jb = (j == 0) ? 2 : j - 1;
-                const dv3 pk = vload(M, comp(p, face_vslot(f, j)));
-                const dv3 pa = vload(M, comp(p, face_vslot(f, ja)));
-                const dv3 pb = vload(M, comp(p, face_vslot(f, jb)));
-                const dv3 cface = cload(&M.fcc[4 * (size_t)tt + (3 - f)]);
-                const int bl = b - b0;
-                const dv3 cv = mk(ws.u.b.vt[bl][0], ws.u.b.vt[bl][1], ws.u.b.vt[bl][2]);
-                const dv3 cqa = tri_cc(pk, q, pa);
-                const dv3 cqb = tri_cc(pk, q, pb);
-                ws.u.b.terms[dest] = -subcell_volume(pk, q, pa, pb, cv, cqa, cqb, cface);
+                const double vol = subcell_volume(pk, pa, pb, pc, ct, f1, f2, f3);
+                term = old_term ? vol : -vol;
             }
-            g.sync();
         }
+        const unsigned peers = g.match(s);
+        const bool lead = s >= 0 && (__ffs(peers) - 1) == g.lane;
+        unsigned rem = lead ? peers : 0u;
+        double a = lead ? ws.acc[s] : 0.0;
+        while (g.any(rem != 0u)) {
+            const int src = rem ? __ffs(rem) - 1 : g.lane;
+            const double tv = g.shfl(term, src);
+            if (rem) {
+                a = fadd(a, tv);
+                rem &= rem - 1u;
+            }
+        }
+        if (lead) ws.acc[s] = a;
         g.sync();
     }
-
-    // per-neighbour sums in natinterp3d's accumulation order
-    for (int s = g.lane; s < nnb; s += G) {
-        double acc = 0.0;
-        const int o = ws.off[s], e = o + ws.cnt[s];
-        for (int j = o; j < e; j++) acc = fadd(acc, ws.u.b.terms[j]);
-        ws.w[s] = acc;
-    }
-    g.sync();
 
     // ---- 5. normalisation -----------------------------------------------------
     double total = 0.0;
     if (g.lane == 0)
-        for (int s = 0; s < nnb; s++) total = fadd(total, ws.w[s]);
+        for (int s = 0; s < nnb; s++) total = fadd(total, ws.acc[s]);
     total = g.shfl(total, 0);
     if (!(total > 1e-30)) return r;  // empty row
     const double inv = fdiv(1.0, total);
-    for (int s = g.lane; s < nnb; s += G) ws.w[s] = fmul(ws.w[s], inv);
+    for (int s = g.lane; s < nnb; s += G) ws.acc[s] = fmul(ws.acc[s], inv);
     g.sync();
     r.nnb = nnb;
     return r;

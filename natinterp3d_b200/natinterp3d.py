@@ -147,12 +147,13 @@ class Interpolator:
         q = self._host_queries(query_points)
         dm = self.device_mesh
         qd = torch.from_numpy(q).to(dm.device)
-        vals_dtype = torch.float32 if out_dtype == np.float32 else torch.float64
-        rowptr, cols, vals = dm.weights_csr(qd, self._centroid, vals_dtype=vals_dtype)
+        rowptr, cols, vals = dm.weights_csr(qd, self._centroid, vals_dtype=torch.float64)
         M = q.shape[0]
         W = scipy.sparse.csr_matrix(
             (vals.cpu().numpy(), cols.cpu().numpy(), rowptr.cpu().numpy()),
             shape=(M, self.n_keys))
+        # natinterp3d.py:117; a dtype-changing astype also canonicalises the
+        # CSR (sorted columns), exactly as it does for natinterp3d's result
         return W.astype(out_dtype, copy=False)
 
     def interpolate(self, query_points: np.ndarray, values: np.ndarray) -> np.ndarray:

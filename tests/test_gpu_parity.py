@@ -97,13 +97,21 @@ def test_lattice_mixture_against_oracle(cuda_device):
     I = ni.Interpolator.from_mesh(c, *arrays)
     W = I.get_weights(q)
     bitwise_csr(W, oracle.OracleMesh(*arrays).weights(q - c))
-    # linear reproduction against the mesh (perturbed) coordinates, interior rows
+    # linear reproduction against the mesh (perturbed) coordinates, for
+    # queries at least 0.01 inside the convex hull: closer to the hull a
+    # super-simplex vertex can be a natural neighbour, whose share natinterp3d
+    # drops before normalising (the flat, clipped faces of the mixture make
+    # that band visible)
+    from scipy.spatial import ConvexHull
     vx = arrays[0][:keys.shape[0]] + c
     a, b = np.array([0.3, -1.2, 2.0]), 0.7
     f = vx @ a + b
     out = I.interpolate(q, f)
-    inner = np.asarray(W.sum(axis=1)).ravel() > 0.5
-    assert np.abs(out[inner] - (q[inner] @ a + b)).max() < 1e-6
+    eq = ConvexHull(vx).equations
+    depth = -(q @ eq[:, :3].T + eq[:, 3]).max(axis=1)
+    deep = depth > 0.01
+    assert deep.sum() > 15000
+    assert np.abs(out[deep] - (q[deep] @ a + b)).max() < 1e-12
 
 
 def test_large_cavities_use_large_kernel(cuda_device):
