@@ -39,6 +39,7 @@ extern "C" {
 #define NIF_ERR_CUDA (-7)       /* a CUDA runtime call failed */
 #define NIF_ERR_CAPACITY (-8)   /* a query exceeded the large kernel's per-query limits */
 #define NIF_ERR_WORKSPACE (-9)  /* a caller buffer is smaller than the queried size */
+#define NIF_ERR_TOO_LARGE (-10) /* more queries than nif_interpolate_noalloc's fixed scratch holds */
 
 /* ---- element types ----------------------------------------------------- */
 #define NIF_F64 0
@@ -172,6 +173,31 @@ int nif_profile_read(double ms[4]);
  * multiply and add -- the latter is the ceiling for the query kernels, which
  * never fuse.  Allocates 8 bytes of device memory for its duration. */
 int nif_measure_fp64_peak(double *tflops_fused, double *tflops_separate);
+
+/* ---- interpolation without any device allocation ------------------------
+ * No counterpart in natinterp3d.  For callers that cannot hand this library a
+ * workspace or let it allocate one: a process whose device memory is already
+ * owned by another pool (a serving framework that reserved the GPU up front),
+ * or a latency-critical loop where a device allocation could fail or quietly
+ * synchronise the whole device.
+ *
+ * Same contract and results as nif_interpolate, minus the workspace
+ * arguments: the scratch lives in a fixed static device array of
+ * NIF_NOALLOC_SCRATCH_BYTES inside libnif_cuda.so, which every GPU that loads
+ * the library keeps until the process exits.  At most NIF_NOALLOC_MAX_QUERIES
+ * queries per call; more return NIF_ERR_TOO_LARGE (split the batch).
+ * The mesh's device must be current.  The first call on each device looks up
+ * the array's device address (a CUDA runtime query, made once per device);
+ * make that first call before any stream capture.  All calls share the one
+ * array and each call re-initialises what must start at zero, so two calls
+ * that can run on the GPU at the same time (different streams, or different
+ * host threads) race on it: serialise them.  Allocates no device or host
+ * memory.  If summary is non-NULL the call synchronises `stream`. */
+#define NIF_NOALLOC_MAX_QUERIES (1 << 20)
+#define NIF_NOALLOC_SCRATCH_BYTES (16u << 20)
+int nif_interpolate_noalloc(const nif_dmesh *m, const void *d_queries, int query_dtype, int64_t M,
+                            const double centroid[3], const void *d_values, int values_dtype, int D,
+                            void *d_out, int out_dtype, void *stream, nif_summary *summary);
 
 #ifdef __cplusplus
 }

@@ -30,6 +30,7 @@ NIF_ERR_WALK = -6
 NIF_ERR_CUDA = -7
 NIF_ERR_CAPACITY = -8
 NIF_ERR_WORKSPACE = -9
+NIF_ERR_TOO_LARGE = -10
 
 _ERR_NAMES = {
     NIF_ERR_ARG: 'invalid argument',
@@ -41,6 +42,7 @@ _ERR_NAMES = {
     NIF_ERR_CUDA: 'CUDA error',
     NIF_ERR_CAPACITY: 'per-query capacity exceeded',
     NIF_ERR_WORKSPACE: 'workspace too small',
+    NIF_ERR_TOO_LARGE: 'more queries than the fixed scratch holds',
 }
 
 
@@ -180,6 +182,9 @@ CUDA_SIGNATURES = {
     'nif_profile_enable': (c_int, [c_int]),
     'nif_profile_read': (c_int, [c_double_p]),
     'nif_measure_fp64_peak': (c_int, [c_double_p, c_double_p]),
+    'nif_interpolate_noalloc': (c_int, [c_void_p, c_void_p, c_int, c_int64, c_double_p, c_void_p,
+                                        c_int, c_int, c_void_p, c_int, c_void_p,
+                                        ctypes.POINTER(Summary)]),
 }
 
 MESH_SIGNATURES = ('nif_mesh_build', 'nif_mesh_free', 'nif_mesh_sizes', 'nif_mesh_export',

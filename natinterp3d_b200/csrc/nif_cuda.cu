@@ -22,6 +22,7 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <mutex>
 #include <new>
 
 #include "natinterp3d_b200.h"
@@ -1135,5 +1136,127 @@ NIF_EXPORT int nif_measure_fp64_peak(double *tflops_fused, double *tflops_separa
     cudaFree(out);
     *tflops_fused = best[0];
     *tflops_separate = best[1];
+    return cuda_rc(cudaGetLastError());
+}
+
+// ===========================================================================
+// Allocation-free interpolation (nif_interpolate_noalloc)
+//
+// For callers that cannot allocate device memory or pass a workspace in: the
+// scratch of one call lives in the static array below, which the CUDA runtime
+// places on every device that loads this library for the life of the process.
+// Host code must never pass the array's name to a kernel -- on the host that
+// name is only a stand-in, not a device address -- so the device address is
+// looked up once per device with cudaGetSymbolAddress and cached.
+// ===========================================================================
+namespace {
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[NIF_NOALLOC_SCRATCH_BYTES];
+
+constexpr int NOALLOC_LARGE_GROUPS = 8;  // large-row workspaces inside the scratch
+constexpr int NOALLOC_MAX_DEVICES = 256;
+
+std::mutex g_noalloc_mu;
+void *g_noalloc_addr[NOALLOC_MAX_DEVICES] = {};
+
+// device address of this device's scratch array, looked up on first use
+int noalloc_scratch(int dev, void **out) {
+    if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) return NIF_ERR_ARG;
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_addr[dev]) {
+        void *p = nullptr;
+        if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return NIF_ERR_CUDA;
+        g_noalloc_addr[dev] = p;
+    }
+    *out = g_noalloc_addr[dev];
+    return NIF_OK;
+}
+
+// interpolate-mode layout with NOALLOC_LARGE_GROUPS large-row workspaces
+QueryLayout carve_noalloc(Carve &c, int64_t M) {
+    QueryLayout L{};
+    const int bits = bucket_bits(M);
+    const int64_t nbk = (int64_t)1 << (3 * bits);
+    const int64_t mscan = M > nbk ? M : nbk;
+    L.sum = c.take<DevSummary>(1);
+    L.bucket = c.take<int>(M > 0 ? M : 1);
+    L.bcount = c.take<int>(nbk + 1);
+    L.order = c.take<int>(M > 0 ? M : 1);
+    L.large_list = c.take<int>(M > 0 ? M : 1);
+    L.scan_bsum = c.take<int64_t>((mscan + SCAN_TILE - 1) / SCAN_TILE + 1);
+    L.scan_total = c.take<int64_t>(1);
+    L.large_ws = c.take<LargeWS>(NOALLOC_LARGE_GROUPS);
+    return L;
+}
+
+template <class QT, class Sink>
+void noalloc_rows(const nif_dmesh *m, const QT *Q, int64_t M, const Centroid &cen,
+                  const QueryLayout &L, const Sink &sink, cudaStream_t st) {
+    constexpr int GPB = FAST_BLOCK / FAST_G;
+    const size_t smem = GPB * sizeof(FastWS);
+    auto kern = k_rows_fast<QT, Sink>;
+    static int per_sm = -1;
+    if (per_sm < 0) {
+        if (smem > 48 * 1024) set_smem(kern, smem);
+        per_sm = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, FAST_BLOCK, smem);
+        if (per_sm < 1) per_sm = 1;
+    }
+    int64_t blocks = (M + GPB - 1) / GPB;
+    const int64_t cap = (int64_t)per_sm * m->num_sms;
+    if (blocks > cap) blocks = cap;
+    if (blocks < 1) blocks = 1;
+    kern<<<(unsigned)blocks, FAST_BLOCK, smem, st>>>(m->view, Q, cen, L.order, M, sink,
+                                                    LargeQueue{L.large_list}, L.sum);
+    k_rows_large<QT, Sink><<<NOALLOC_LARGE_GROUPS, 32, 0, st>>>(
+        m->view, Q, cen, LargeQueue{L.large_list}, sink, L.large_ws, L.sum);
+}
+
+template <class QT, class VT, class CT>
+void noalloc_typed(const nif_dmesh *m, const void *q, int64_t M, const Centroid &cen,
+                   const void *v, int D, void *out, const QueryLayout &L, cudaStream_t st) {
+    InterpSink<QT, VT, CT> sink{static_cast<const VT *>(v), static_cast<CT *>(out), D};
+    run_bucketing(m, static_cast<const QT *>(q), M, cen, L, st);
+    noalloc_rows(m, static_cast<const QT *>(q), M, cen, L, sink, st);
+}
+
+}  // namespace
+
+NIF_EXPORT int nif_interpolate_noalloc(const nif_dmesh *m, const void *d_queries, int query_dtype,
+                                       int64_t M, const double centroid[3], const void *d_values,
+                                       int values_dtype, int D, void *d_out, int out_dtype,
+                                       void *stream, nif_summary *summary) {
+    if (!m || !centroid || M < 0) return NIF_ERR_ARG;
+    if (M > (int64_t)NIF_NOALLOC_MAX_QUERIES) return NIF_ERR_TOO_LARGE;
+    if (query_dtype != NIF_F64 && query_dtype != NIF_F32) return NIF_ERR_ARG;
+    if (values_dtype != NIF_F64 && values_dtype != NIF_F32) return NIF_ERR_ARG;
+    if (D < 1) return NIF_ERR_ARG;
+    const int expect = (query_dtype == NIF_F32 && values_dtype == NIF_F32) ? NIF_F32 : NIF_F64;
+    if (out_dtype != expect) return NIF_ERR_ARG;
+    if (M > 0 && (!d_queries || !d_values || !d_out)) return NIF_ERR_ARG;
+    int dev = -1;
+    NIF_CUDA(cudaGetDevice(&dev));
+    if (dev != m->device) return NIF_ERR_ARG;
+    void *scratch = nullptr;
+    int rc = noalloc_scratch(dev, &scratch);
+    if (rc != NIF_OK) return rc;
+    Carve c{reinterpret_cast<unsigned char *>(scratch), 0, NIF_NOALLOC_SCRATCH_BYTES, true};
+    QueryLayout L = carve_noalloc(c, M);
+    if (!c.ok) return NIF_ERR_INTERNAL;  // the fixed array must hold the largest accepted call
+    cudaStream_t st = S(stream);
+    Centroid cen{{centroid[0], centroid[1], centroid[2]}};
+    // counters and queue length start at zero (bucket counts are cleared by run_bucketing)
+    NIF_CUDA(cudaMemsetAsync(L.sum, 0, sizeof(DevSummary), st));
+    if (M > 0) {
+        if (query_dtype == NIF_F64 && values_dtype == NIF_F64)
+            noalloc_typed<double, double, double>(m, d_queries, M, cen, d_values, D, d_out, L, st);
+        else if (query_dtype == NIF_F64)
+            noalloc_typed<double, float, double>(m, d_queries, M, cen, d_values, D, d_out, L, st);
+        else if (values_dtype == NIF_F32)
+            noalloc_typed<float, float, float>(m, d_queries, M, cen, d_values, D, d_out, L, st);
+        else
+            noalloc_typed<float, double, double>(m, d_queries, M, cen, d_values, D, d_out, L, st);
+    }
+    if (summary) return read_summary(L, st, summary, nullptr);
     return cuda_rc(cudaGetLastError());
 }
