@@ -352,7 +352,11 @@ def main():
                 'phase_ms': {'bucketing': float(np.mean(kms[:, 0])), 'rows_fast': rows_ms,
                              'rows_large': float(np.mean(kms[:, 2])),
                              'epilogue': float(np.mean(kms[:, 3]))},
-                'traffic': None,
+                # dram__bytes_read.sum + dram__bytes_write.sum of one k_rows_fast launch at
+                # 200k keys / 2M queries (profiles/k_rows_fast_200k_keys_2M_queries.md),
+                # scaled by this launch's queries (the mesh scales with the keys alike)
+                'traffic': 802.0e6 * (M / 2_000_000),
+                'traffic_note': 'ncu capture at 200k keys / 2M queries scaled by queries',
             },
             'cpu_baseline': cpu,
             'e2e': {'value': M * world / e2e_sec, 'unit': 'queries/s',
