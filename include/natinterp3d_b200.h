@@ -160,6 +160,37 @@ int nif_interpolate(const nif_dmesh *m, const void *d_queries, int query_dtype, 
                     void *d_out, int out_dtype, void *d_ws, size_t ws_bytes, void *stream,
                     nif_summary *summary);
 
+/* ---- differentiable path (no counterpart in natinterp3d) ----------------- */
+
+/* y[M][D] = W x with W an M-row CSR (int32 row pointers and columns) and
+ * x [N][D]: each y[i, d] accumulated from zero over the row's entries in
+ * stored order, in the promoted type -- what scipy's `W @ x` computes
+ * (natinterp3d.py:131-137).  y_dtype must be promote(vals_dtype, x_dtype). */
+int nif_spmm(int64_t M, int64_t N, const int32_t *d_rowptr, const int32_t *d_cols,
+             const void *d_vals, int vals_dtype, const void *d_x, int x_dtype, int D, void *d_y,
+             int y_dtype, void *stream);
+
+/* y[N][D] = W^T x for x [M][D]: the gradient of `W @ values` with respect to
+ * values.  Deterministic: a CSC is built by a stable radix sort of the
+ * columns (no floating-point atomics) and each y[k, d] is accumulated from
+ * zero in ascending row order.  Workspace size from nif_spmm_t_workspace_bytes. */
+int nif_spmm_t_workspace_bytes(int64_t M, int64_t N, int64_t nnz, size_t *bytes);
+int nif_spmm_t(int64_t M, int64_t N, int64_t nnz, const int32_t *d_rowptr, const int32_t *d_cols,
+               const void *d_vals, int vals_dtype, const void *d_x, int x_dtype, int D, void *d_y,
+               int y_dtype, void *d_ws, size_t ws_bytes, void *stream);
+
+/* Gradient of a loss through interpolation with respect to the query
+ * positions: gq[i, :] = sum_k (gout[i, :] . values[k, :]) dw_ik/dq_i, from the
+ * analytic derivative of every stolen volume (the virtual-tet terms of
+ * natural_insertionfree.c:681-719; all other terms are locally constant),
+ * recomputing each query's cavity.  gout_dtype = promote(query, values);
+ * gq has the query dtype; rows without a derivative (empty, or exactly on a
+ * data site) get zero.  Workspace: nif_query_workspace_bytes(NIF_MODE_INTERP). */
+int nif_query_grad(const nif_dmesh *m, const void *d_queries, int query_dtype, int64_t M,
+                   const double centroid[3], const void *d_values, int values_dtype, int D,
+                   const void *d_gout, int gout_dtype, void *d_gq, void *d_ws, size_t ws_bytes,
+                   void *stream, nif_summary *summary);
+
 /* Measurement.  While enabled, every query call records CUDA events on its
  * stream between its phases; nif_profile_read waits for the last call's
  * final event and returns the device time in milliseconds of

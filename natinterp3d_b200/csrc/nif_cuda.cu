@@ -23,10 +23,12 @@
 #include <string.h>
 
 #include <mutex>
+#include <type_traits>
 #include <new>
 
 #include "natinterp3d_b200.h"
 #include "nif_kernels.cuh"
+#include "nif_grad.cuh"
 
 #define NIF_EXPORT extern "C" __attribute__((visibility("default")))
 
@@ -348,8 +350,8 @@ struct StageSink {
     DevSummary *sum;
 
     template <int G, class W>
-    __device__ __forceinline__ void emit(int64_t i, int nnb, const W &ws, const Grp<G> &g,
-                                         bool large) {
+    __device__ __forceinline__ void emit(int64_t i, int nnb, W &ws, const Grp<G> &g, bool large,
+                                         const MeshView &, dv3, const RowInfo &) {
         int64_t o = i * ROW_CAP;
         if (large) {
             unsigned long long a = 0;
@@ -406,7 +408,8 @@ struct InterpSink {
     static constexpr bool SORTED = sizeof(WT) == 4;
 
     template <int G, class W>
-    __device__ __forceinline__ void emit(int64_t i, int nnb, W &ws, const Grp<G> &g, bool) {
+    __device__ __forceinline__ void emit(int64_t i, int nnb, W &ws, const Grp<G> &g, bool,
+                                         const MeshView &, dv3, const RowInfo &) {
         CT *o = out + i * (int64_t)D;
         if (nnb == 0) {
             for (int d = g.lane; d < D; d += G) o[d] = (CT)0;
@@ -451,6 +454,238 @@ struct InterpSink {
     }
 };
 
+// d loss / d query: gq[i, :] = sum_k dL/dw_ik dw_ik/dq_i with dL/dw_ik =
+// gout[i, :] . values[k, :] (derivation in nif_grad.cuh).  Rows without a
+// well-defined derivative (empty, outside the super-simplex, or exactly on
+// a data site, where Sibson coordinates are only continuous) get zero.
+template <class QT, class VT, class GT>
+struct GradSink {
+    const VT *__restrict__ values;  // [N][D]
+    const GT *__restrict__ gout;    // [M][D]
+    QT *__restrict__ gq;            // [M][3]
+    int D;
+
+    template <int G, class W>
+    __device__ __forceinline__ void emit(int64_t i, int nnb, W &ws, const Grp<G> &g, bool,
+                                         const MeshView &M, dv3 q, const RowInfo &r) {
+        double gx = 0.0, gy = 0.0, gz = 0.0;
+        if (nnb > 0 && !r.coincident && r.total > 0.0) {
+            double *gk = reinterpret_cast<double *>(&ws.u);  // free after the cavity search
+            const GT *go = gout + i * (int64_t)D;
+            for (int s = g.lane; s < nnb; s += G) {
+                const VT *vr = values + (int64_t)ws.nbr_vid[s] * D;
+                double a = 0.0;
+                for (int d = 0; d < D; d++) a += (double)go[d] * (double)vr[d];
+                gk[s] = a;
+            }
+            g.sync();
+            double gbar = 0.0;
+            if (g.lane == 0)
+                for (int s = 0; s < nnb; s++) gbar += gk[s] * ws.acc[s];
+            gbar = g.shfl(gbar, 0);
+            const double inv_total = 1.0 / r.total;
+            for (int s = g.lane; s < nnb; s += G) gk[s] = (gk[s] - gbar) * inv_total;
+            g.sync();
+            for (int k = g.lane; k < 3 * r.nbf; k += G) {
+                const int b = k / 3, j = k - 3 * b;
+                const int cf = ws.bface[b];
+                const int f = cf & 3;
+                const int tt = ws.cav_tet[cf >> 2];
+                const int4 p = M.tv[tt];
+                const int va = comp(p, face_vslot(f, 0));
+                const int vb = comp(p, face_vslot(f, 1));
+                const int vc = comp(p, face_vslot(f, 2));
+                const int v = (j == 0) ? va : (j == 1 ? vb : vc);
+                if (v >= M.n) continue;
+                const int s = neighbour_slot(ws, v);
+                if (s < 0) continue;
+                const dv3 dvol = virtual_term_grad(q, vload(M, va), vload(M, vb), vload(M, vc),
+                                                   cload(&M.fcc[4 * (size_t)tt + (3 - f)]), j);
+                // virtual terms enter the stolen volume with a minus sign
+                const double c = gk[s];
+                gx -= c * dvol.x;
+                gy -= c * dvol.y;
+                gz -= c * dvol.z;
+            }
+#pragma unroll
+            for (int o = G / 2; o > 0; o >>= 1) {
+                gx += __shfl_xor_sync(g.mask, gx, o, G);
+                gy += __shfl_xor_sync(g.mask, gy, o, G);
+                gz += __shfl_xor_sync(g.mask, gz, o, G);
+            }
+            g.sync();
+        }
+        if (g.lane == 0) {
+            gq[3 * i] = (QT)gx;
+            gq[3 * i + 1] = (QT)gy;
+            gq[3 * i + 2] = (QT)gz;
+        }
+    }
+};
+
+// ---------------------------------------------------------------------------
+// sparse products: CSR x dense and its transpose through a sorted CSC
+// ---------------------------------------------------------------------------
+
+// y[i, d] = sum over row i of w * x[col, d], accumulated from zero in stored
+// order in the promoted type (scipy csr_matvecs)
+template <class WT, class XT, class CT>
+__global__ void k_spmm(int64_t M, int D, const int32_t *__restrict__ rowptr,
+                       const int32_t *__restrict__ cols, const WT *__restrict__ vals,
+                       const XT *__restrict__ x, CT *__restrict__ y) {
+    for (int64_t u = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; u < M * D;
+         u += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = u / D;
+        const int d = (int)(u - i * D);
+        CT acc = (CT)0;
+        for (int e = rowptr[i]; e < rowptr[i + 1]; e++)
+            acc = Arith<CT>::add(acc, Arith<CT>::mul((CT)vals[e], (CT)x[(int64_t)cols[e] * D + d]));
+        y[u] = acc;
+    }
+}
+
+__global__ void k_row_of(int64_t M, const int32_t *__restrict__ rowptr, int32_t *__restrict__ rowof,
+                         uint32_t *__restrict__ keys, const int32_t *__restrict__ cols,
+                         int32_t *__restrict__ idx) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < M;
+         i += (int64_t)gridDim.x * blockDim.x)
+        for (int e = rowptr[i]; e < rowptr[i + 1]; e++) {
+            rowof[e] = (int32_t)i;
+            keys[e] = (uint32_t)cols[e];
+            idx[e] = e;
+        }
+}
+
+// stable LSD radix sort of (key, value) pairs, 4 bits per pass
+constexpr int RS_THREADS = 256;
+constexpr int RS_ITEMS = 8;
+constexpr int RS_TILE = RS_THREADS * RS_ITEMS;
+
+__global__ void __launch_bounds__(RS_THREADS) k_rs_hist(const uint32_t *__restrict__ keys, int64_t n,
+                                                         int shift, int nblocks, int *__restrict__ hist) {
+    __shared__ int h[16];
+    if (threadIdx.x < 16) h[threadIdx.x] = 0;
+    __syncthreads();
+    const int64_t base = (int64_t)blockIdx.x * RS_TILE;
+    for (int j = 0; j < RS_ITEMS; j++) {
+        const int64_t i = base + j * RS_THREADS + threadIdx.x;
+        if (i < n) atomicAdd(&h[(keys[i] >> shift) & 15u], 1);
+    }
+    __syncthreads();
+    if (threadIdx.x < 16) hist[(int64_t)threadIdx.x * nblocks + blockIdx.x] = h[threadIdx.x];
+}
+
+__device__ __forceinline__ unsigned long long pick4(unsigned long long c0, unsigned long long c1,
+                                                    unsigned long long c2, unsigned long long c3,
+                                                    int d) {
+    const unsigned long long c = (d < 4) ? c0 : (d < 8 ? c1 : (d < 12 ? c2 : c3));
+    return (c >> (16 * (d & 3))) & 0xffffull;
+}
+
+// Thread t of a block owns the tile's items 8t..8t+7 in order; an item's
+// destination is the block's start for its digit (scanned histogram) plus
+// the digit's count in earlier threads plus its rank inside its own thread,
+// so equal keys keep their input order.  Counts are packed 16 bits per digit.
+__global__ void __launch_bounds__(RS_THREADS) k_rs_scatter(
+    const uint32_t *__restrict__ kin, const int32_t *__restrict__ vin, int64_t n, int shift,
+    int nblocks, const int *__restrict__ off, uint32_t *__restrict__ kout, int32_t *__restrict__ vout) {
+    __shared__ uint32_t sk[RS_TILE];
+    __shared__ int32_t sv[RS_TILE];
+    __shared__ unsigned long long wsum[RS_THREADS / 32][4];
+    const int64_t base = (int64_t)blockIdx.x * RS_TILE;
+    for (int j = 0; j < RS_ITEMS; j++) {
+        const int idx = j * RS_THREADS + threadIdx.x;
+        if (base + idx < n) {
+            sk[idx] = kin[base + idx];
+            sv[idx] = vin[base + idx];
+        }
+    }
+    __syncthreads();
+    uint32_t mk[RS_ITEMS];
+    int32_t mv[RS_ITEMS];
+    int dg[RS_ITEMS], rk[RS_ITEMS];
+    unsigned long long c0 = 0, c1 = 0, c2 = 0, c3 = 0;
+#pragma unroll
+    for (int j = 0; j < RS_ITEMS; j++) {
+        const int idx = threadIdx.x * RS_ITEMS + j;
+        dg[j] = -1;
+        rk[j] = 0;
+        mk[j] = 0;
+        mv[j] = 0;
+        if (base + idx < n) {
+            mk[j] = sk[idx];
+            mv[j] = sv[idx];
+            const int d = (int)((mk[j] >> shift) & 15u);
+            dg[j] = d;
+            rk[j] = (int)pick4(c0, c1, c2, c3, d);
+            const unsigned long long inc = 1ull << (16 * (d & 3));
+            if (d < 4) c0 += inc; else if (d < 8) c1 += inc; else if (d < 12) c2 += inc; else c3 += inc;
+        }
+    }
+    // exclusive scan of the packed counts over the block's threads
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    unsigned long long s0 = c0, s1 = c1, s2 = c2, s3 = c3;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned long long t0 = __shfl_up_sync(0xffffffffu, s0, o);
+        const unsigned long long t1 = __shfl_up_sync(0xffffffffu, s1, o);
+        const unsigned long long t2 = __shfl_up_sync(0xffffffffu, s2, o);
+        const unsigned long long t3 = __shfl_up_sync(0xffffffffu, s3, o);
+        if (lane >= o) {
+            s0 += t0; s1 += t1; s2 += t2; s3 += t3;
+        }
+    }
+    if (lane == 31) {
+        wsum[warp][0] = s0; wsum[warp][1] = s1; wsum[warp][2] = s2; wsum[warp][3] = s3;
+    }
+    __syncthreads();
+    unsigned long long e0 = s0 - c0, e1 = s1 - c1, e2 = s2 - c2, e3 = s3 - c3;
+    for (int w = 0; w < warp; w++) {
+        e0 += wsum[w][0]; e1 += wsum[w][1]; e2 += wsum[w][2]; e3 += wsum[w][3];
+    }
+#pragma unroll
+    for (int j = 0; j < RS_ITEMS; j++) {
+        const int d = dg[j];
+        if (d < 0) continue;
+        const int64_t pos = (int64_t)off[(int64_t)d * nblocks + blockIdx.x] +
+                            (int64_t)pick4(e0, e1, e2, e3, d) + rk[j];
+        kout[pos] = mk[j];
+        vout[pos] = mv[j];
+    }
+}
+
+// colptr[k] = first position of key k in the sorted keys (lower bound)
+__global__ void k_colptr(const uint32_t *__restrict__ keys, int64_t n, int64_t N,
+                         int32_t *__restrict__ colptr) {
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k <= N;
+         k += (int64_t)gridDim.x * blockDim.x) {
+        int64_t lo = 0, hi = n;
+        while (lo < hi) {
+            const int64_t mid = (lo + hi) >> 1;
+            if ((int64_t)keys[mid] < k) lo = mid + 1; else hi = mid;
+        }
+        colptr[k] = (int32_t)lo;
+    }
+}
+
+// y[k, d] = sum over column k, ascending row, of w * x[row, d]
+template <class WT, class XT, class CT>
+__global__ void k_spmm_t(int64_t N, int D, const int32_t *__restrict__ colptr,
+                         const int32_t *__restrict__ perm, const int32_t *__restrict__ rowof,
+                         const WT *__restrict__ vals, const XT *__restrict__ x, CT *__restrict__ y) {
+    for (int64_t u = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; u < N * D;
+         u += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t k = u / D;
+        const int d = (int)(u - k * D);
+        CT acc = (CT)0;
+        for (int p = colptr[k]; p < colptr[k + 1]; p++) {
+            const int e = perm[p];
+            acc = Arith<CT>::add(acc, Arith<CT>::mul((CT)vals[e], (CT)x[(int64_t)rowof[e] * D + d]));
+        }
+        y[u] = acc;
+    }
+}
+
 // ---------------------------------------------------------------------------
 // row kernels
 // ---------------------------------------------------------------------------
@@ -494,7 +729,7 @@ __global__ void __launch_bounds__(FAST_BLOCK, NIF_FAST_MINB) k_rows_fast(MeshVie
                 atomicCAS(&sum->first_status, 0, NIF_ERR_WALK);
             }
             record<G>(sum, r, g.lane);
-            sink.template emit<G>(i, r.status == ST_OK ? r.nnb : 0, ws, g, false);
+            sink.template emit<G>(i, r.status == ST_OK ? r.nnb : 0, ws, g, false, M, q, r);
         }
         g.sync();
     }
@@ -523,10 +758,10 @@ __global__ void __launch_bounds__(32) k_rows_large(MeshView M, const QT *__restr
                 atomicCAS(&sum->first_status, 0,
                           r.status == ST_WALK ? NIF_ERR_WALK : NIF_ERR_CAPACITY);
             }
-            sink.template emit<G>(i, 0, ws, g, true);
+            sink.template emit<G>(i, 0, ws, g, true, M, q, r);
         } else {
             record<G>(sum, r, g.lane);
-            sink.template emit<G>(i, r.nnb, ws, g, true);
+            sink.template emit<G>(i, r.nnb, ws, g, true, M, q, r);
         }
         g.sync();
     }
@@ -1256,6 +1491,175 @@ NIF_EXPORT int nif_interpolate_noalloc(const nif_dmesh *m, const void *d_queries
             noalloc_typed<float, float, float>(m, d_queries, M, cen, d_values, D, d_out, L, st);
         else
             noalloc_typed<float, double, double>(m, d_queries, M, cen, d_values, D, d_out, L, st);
+    }
+    if (summary) return read_summary(L, st, summary, nullptr);
+    return cuda_rc(cudaGetLastError());
+}
+
+// ===========================================================================
+// sparse products and the query gradient
+// ===========================================================================
+namespace {
+
+template <class WT, class XT>
+int spmm_typed(int64_t M, int D, const int32_t *rowptr, const int32_t *cols, const void *vals,
+               const void *x, void *y, cudaStream_t st) {
+    using CT = typename std::conditional<(sizeof(WT) == 8 || sizeof(XT) == 8), double, float>::type;
+    if (M * D == 0) return NIF_OK;
+    k_spmm<WT, XT, CT><<<blocks_for(M * D, 256), 256, 0, st>>>(
+        M, D, rowptr, cols, static_cast<const WT *>(vals), static_cast<const XT *>(x),
+        static_cast<CT *>(y));
+    return cuda_rc(cudaGetLastError());
+}
+
+template <class WT, class XT>
+int spmm_t_typed(int64_t N, int D, const int32_t *colptr, const int32_t *perm, const int32_t *rowof,
+                 const void *vals, const void *x, void *y, cudaStream_t st) {
+    using CT = typename std::conditional<(sizeof(WT) == 8 || sizeof(XT) == 8), double, float>::type;
+    if (N * D == 0) return NIF_OK;
+    k_spmm_t<WT, XT, CT><<<blocks_for(N * D, 256), 256, 0, st>>>(
+        N, D, colptr, perm, rowof, static_cast<const WT *>(vals), static_cast<const XT *>(x),
+        static_cast<CT *>(y));
+    return cuda_rc(cudaGetLastError());
+}
+
+int expect_promoted(int a, int b) { return (a == NIF_F32 && b == NIF_F32) ? NIF_F32 : NIF_F64; }
+
+struct CscLayout {
+    int32_t *rowof, *idx_a, *idx_b, *colptr;
+    uint32_t *key_a, *key_b;
+    int *hist, *off, *bsum, *total;
+};
+
+CscLayout carve_csc(Carve &c, int64_t nnz, int64_t N) {
+    CscLayout L{};
+    const int64_t nb = (nnz + RS_TILE - 1) / RS_TILE;
+    const int64_t nh = 16 * (nb > 0 ? nb : 1);
+    L.rowof = c.take<int32_t>(nnz > 0 ? nnz : 1);
+    L.idx_a = c.take<int32_t>(nnz > 0 ? nnz : 1);
+    L.idx_b = c.take<int32_t>(nnz > 0 ? nnz : 1);
+    L.key_a = c.take<uint32_t>(nnz > 0 ? nnz : 1);
+    L.key_b = c.take<uint32_t>(nnz > 0 ? nnz : 1);
+    L.colptr = c.take<int32_t>(N + 1);
+    L.hist = c.take<int>(nh);
+    L.off = c.take<int>(nh);
+    L.bsum = c.take<int>((nh + SCAN_TILE - 1) / SCAN_TILE + 1);
+    L.total = c.take<int>(2);
+    return L;
+}
+
+}  // namespace
+
+NIF_EXPORT int nif_spmm(int64_t M, int64_t N, const int32_t *d_rowptr, const int32_t *d_cols,
+                        const void *d_vals, int vals_dtype, const void *d_x, int x_dtype, int D,
+                        void *d_y, int y_dtype, void *stream) {
+    if (M < 0 || N < 0 || D < 1) return NIF_ERR_ARG;
+    if ((vals_dtype != NIF_F64 && vals_dtype != NIF_F32) || (x_dtype != NIF_F64 && x_dtype != NIF_F32))
+        return NIF_ERR_ARG;
+    if (y_dtype != expect_promoted(vals_dtype, x_dtype)) return NIF_ERR_ARG;
+    if (M > 0 && (!d_rowptr || !d_y)) return NIF_ERR_ARG;
+    cudaStream_t st = S(stream);
+    if (vals_dtype == NIF_F64 && x_dtype == NIF_F64)
+        return spmm_typed<double, double>(M, D, d_rowptr, d_cols, d_vals, d_x, d_y, st);
+    if (vals_dtype == NIF_F64)
+        return spmm_typed<double, float>(M, D, d_rowptr, d_cols, d_vals, d_x, d_y, st);
+    if (x_dtype == NIF_F64)
+        return spmm_typed<float, double>(M, D, d_rowptr, d_cols, d_vals, d_x, d_y, st);
+    return spmm_typed<float, float>(M, D, d_rowptr, d_cols, d_vals, d_x, d_y, st);
+}
+
+NIF_EXPORT int nif_spmm_t_workspace_bytes(int64_t M, int64_t N, int64_t nnz, size_t *bytes) {
+    if (!bytes || M < 0 || N < 0 || nnz < 0 || nnz > (int64_t)INT32_MAX || N >= ((int64_t)1 << 32))
+        return NIF_ERR_ARG;
+    Carve c{nullptr, 0, (size_t)-1, true};
+    carve_csc(c, nnz, N);
+    *bytes = align_up(c.off, 256);
+    return NIF_OK;
+}
+
+NIF_EXPORT int nif_spmm_t(int64_t M, int64_t N, int64_t nnz, const int32_t *d_rowptr,
+                          const int32_t *d_cols, const void *d_vals, int vals_dtype, const void *d_x,
+                          int x_dtype, int D, void *d_y, int y_dtype, void *d_ws, size_t ws_bytes,
+                          void *stream) {
+    size_t need = 0;
+    int rc = nif_spmm_t_workspace_bytes(M, N, nnz, &need);
+    if (rc != NIF_OK) return rc;
+    if (D < 1 || (vals_dtype != NIF_F64 && vals_dtype != NIF_F32) ||
+        (x_dtype != NIF_F64 && x_dtype != NIF_F32) || y_dtype != expect_promoted(vals_dtype, x_dtype))
+        return NIF_ERR_ARG;
+    if (!d_ws || reinterpret_cast<uintptr_t>(d_ws) % 256 != 0) return NIF_ERR_ARG;
+    if (ws_bytes < need) return NIF_ERR_WORKSPACE;
+    if (N > 0 && !d_y) return NIF_ERR_ARG;
+    if (nnz > 0 && (!d_rowptr || !d_cols || !d_vals || !d_x)) return NIF_ERR_ARG;
+    cudaStream_t st = S(stream);
+    Carve c{reinterpret_cast<unsigned char *>(d_ws), 0, ws_bytes, true};
+    CscLayout L = carve_csc(c, nnz, N);
+    if (M > 0)
+        k_row_of<<<blocks_for(M, 256), 256, 0, st>>>(M, d_rowptr, L.rowof, L.key_a, d_cols, L.idx_a);
+    // stable sort by column over as many 4-bit digits as the column count needs
+    int bits = 0;
+    while (bits < 32 && ((int64_t)1 << bits) < N) bits++;
+    const int passes = (bits + 3) / 4;
+    uint32_t *kin = L.key_a, *kout = L.key_b;
+    int32_t *vin = L.idx_a, *vout = L.idx_b;
+    const int64_t nblocks = (nnz + RS_TILE - 1) / RS_TILE;
+    for (int pass = 0; pass < passes && nnz > 0; pass++) {
+        const int shift = 4 * pass;
+        k_rs_hist<<<(unsigned)nblocks, RS_THREADS, 0, st>>>(kin, nnz, shift, (int)nblocks, L.hist);
+        launch_scan<int>(L.hist, 16 * nblocks, L.bsum, L.total, L.off, st);
+        k_rs_scatter<<<(unsigned)nblocks, RS_THREADS, 0, st>>>(kin, vin, nnz, shift, (int)nblocks,
+                                                                L.off, kout, vout);
+        uint32_t *tk = kin; kin = kout; kout = tk;
+        int32_t *tv = vin; vin = vout; vout = tv;
+    }
+    k_colptr<<<blocks_for(N + 1, 256), 256, 0, st>>>(kin, nnz, N, L.colptr);
+    if (vals_dtype == NIF_F64 && x_dtype == NIF_F64)
+        return spmm_t_typed<double, double>(N, D, L.colptr, vin, L.rowof, d_vals, d_x, d_y, st);
+    if (vals_dtype == NIF_F64)
+        return spmm_t_typed<double, float>(N, D, L.colptr, vin, L.rowof, d_vals, d_x, d_y, st);
+    if (x_dtype == NIF_F64)
+        return spmm_t_typed<float, double>(N, D, L.colptr, vin, L.rowof, d_vals, d_x, d_y, st);
+    return spmm_t_typed<float, float>(N, D, L.colptr, vin, L.rowof, d_vals, d_x, d_y, st);
+}
+
+namespace {
+template <class QT, class VT>
+void grad_typed(const nif_dmesh *m, const void *q, int64_t M, const Centroid &cen, const void *v,
+                int D, const void *gout, void *gq, const QueryLayout &L, cudaStream_t st) {
+    using GT = typename std::conditional<(sizeof(QT) == 8 || sizeof(VT) == 8), double, float>::type;
+    GradSink<QT, VT, GT> sink{static_cast<const VT *>(v), static_cast<const GT *>(gout),
+                              static_cast<QT *>(gq), D};
+    run_bucketing(m, static_cast<const QT *>(q), M, cen, L, st);
+    run_rows(m, static_cast<const QT *>(q), M, cen, L, sink, st);
+}
+}  // namespace
+
+NIF_EXPORT int nif_query_grad(const nif_dmesh *m, const void *d_queries, int query_dtype, int64_t M,
+                              const double centroid[3], const void *d_values, int values_dtype,
+                              int D, const void *d_gout, int gout_dtype, void *d_gq, void *d_ws,
+                              size_t ws_bytes, void *stream, nif_summary *summary) {
+    int rc = check_query_args(m, d_queries, query_dtype, M, centroid, d_ws);
+    if (rc != NIF_OK) return rc;
+    if ((values_dtype != NIF_F64 && values_dtype != NIF_F32) || D < 1) return NIF_ERR_ARG;
+    if (gout_dtype != expect_promoted(query_dtype, values_dtype)) return NIF_ERR_ARG;
+    if (M > 0 && (!d_values || !d_gout || !d_gq)) return NIF_ERR_ARG;
+    size_t need = 0;
+    nif_query_workspace_bytes(m, M, NIF_MODE_INTERP, &need);
+    if (ws_bytes < need) return NIF_ERR_WORKSPACE;
+    cudaStream_t st = S(stream);
+    Carve c{reinterpret_cast<unsigned char *>(d_ws), 0, ws_bytes, true};
+    QueryLayout L = carve_query(c, M, NIF_MODE_INTERP);
+    Centroid cen{{centroid[0], centroid[1], centroid[2]}};
+    NIF_CUDA(cudaMemsetAsync(L.sum, 0, sizeof(DevSummary), st));
+    if (M > 0) {
+        if (query_dtype == NIF_F64 && values_dtype == NIF_F64)
+            grad_typed<double, double>(m, d_queries, M, cen, d_values, D, d_gout, d_gq, L, st);
+        else if (query_dtype == NIF_F64)
+            grad_typed<double, float>(m, d_queries, M, cen, d_values, D, d_gout, d_gq, L, st);
+        else if (values_dtype == NIF_F32)
+            grad_typed<float, float>(m, d_queries, M, cen, d_values, D, d_gout, d_gq, L, st);
+        else
+            grad_typed<float, double>(m, d_queries, M, cen, d_values, D, d_gout, d_gq, L, st);
     }
     if (summary) return read_summary(L, st, summary, nullptr);
     return cuda_rc(cudaGetLastError());

@@ -203,6 +203,9 @@ struct RowInfo {
     int nnb;
     int steps;
     bool outside;
+    bool coincident;  // row from the coincident-vertex path
+    double total;     // sum of the stolen volumes (the normaliser), 0 if none
+    int nbf;          // boundary faces (ws.bface[0..nbf))
 };
 
 // Circumcentre natinterp3d's face cache returns for the face opposite p[i] of
@@ -233,7 +236,7 @@ template <int G, class W>
 __device__ RowInfo sibson_row(const MeshView &M, const dv3 q, W &ws, const Grp<G> &g) {
     using cav_t = typename W::cav_t;
     using slot_t = typename W::slot_t;
-    RowInfo r{ST_OK, 0, 0, false};
+    RowInfo r{ST_OK, 0, 0, false, false, 0.0, 0};
 
     // ---- 1. point location -------------------------------------------------
     int t = M.grid[seed_cell(M, q)];
@@ -350,6 +353,7 @@ __device__ RowInfo sibson_row(const MeshView &M, const dv3 q, W &ws, const Grp<G
         }
         g.sync();
         r.nnb = nco;
+        r.coincident = true;
         return r;
     }
 
@@ -425,6 +429,7 @@ __device__ RowInfo sibson_row(const MeshView &M, const dv3 q, W &ws, const Grp<G
         r.status = ST_CAPACITY;
         return r;
     }
+    r.nbf = nbf;
 
     // natural neighbours in first-seen order over the boundary-face vertices
     for (int i = g.lane; i < W::VH; i += G) {
@@ -573,6 +578,7 @@ __device__ RowInfo sibson_row(const MeshView &M, const dv3 q, W &ws, const Grp<G
     for (int s = g.lane; s < nnb; s += G) ws.acc[s] = fmul(ws.acc[s], inv);
     g.sync();
     r.nnb = nnb;
+    r.total = total;
     return r;
 }
 

@@ -149,6 +149,58 @@ class DeviceMesh:
             return out, summ.as_dict()
         return out
 
+    # -------------------------------------------------------------- sparse / grad
+    def spmm(self, rowptr, cols, vals, x):
+        """W @ x for a device CSR W (rows = len(rowptr) - 1, columns = n_keys)."""
+        x2 = x.reshape(x.shape[0], -1).contiguous()
+        M, D = int(rowptr.numel()) - 1, int(x2.shape[1])
+        out_dtype = torch.float32 if (vals.dtype == torch.float32 and x2.dtype == torch.float32) \
+            else torch.float64
+        y = torch.empty((M, D), dtype=out_dtype, device=self.device)
+        with torch.cuda.device(self.device):
+            N.check(self._lib.nif_spmm(M, int(x2.shape[0]), _vp(rowptr), _vp(cols), _vp(vals),
+                                       _DT[vals.dtype], _vp(x2), _DT[x2.dtype], D, _vp(y),
+                                       _DT[out_dtype], _stream_ptr(self.device)), 'nif_spmm')
+        return y
+
+    def spmm_t(self, rowptr, cols, vals, x, n_cols):
+        """W^T @ x (deterministic, CSC by stable sort) for a device CSR W."""
+        x2 = x.reshape(x.shape[0], -1).contiguous()
+        M, D, nnz = int(rowptr.numel()) - 1, int(x2.shape[1]), int(cols.numel())
+        out_dtype = torch.float32 if (vals.dtype == torch.float32 and x2.dtype == torch.float32) \
+            else torch.float64
+        y = torch.empty((n_cols, D), dtype=out_dtype, device=self.device)
+        nb = ctypes.c_size_t()
+        N.check(self._lib.nif_spmm_t_workspace_bytes(M, n_cols, nnz, ctypes.byref(nb)),
+                'nif_spmm_t_workspace_bytes')
+        with torch.cuda.device(self.device):
+            ws = torch.empty(max(int(nb.value), 256), dtype=torch.uint8, device=self.device)
+            N.check(self._lib.nif_spmm_t(M, n_cols, nnz, _vp(rowptr), _vp(cols), _vp(vals),
+                                         _DT[vals.dtype], _vp(x2), _DT[x2.dtype], D, _vp(y),
+                                         _DT[out_dtype], _vp(ws), ws.numel(),
+                                         _stream_ptr(self.device)), 'nif_spmm_t')
+        return y
+
+    def query_grad(self, q, values, gout, centroid):
+        """d loss / d queries for gout = d loss / d interpolate(q, values)."""
+        q = q.contiguous()
+        v = values.reshape(self.n_keys, -1).contiguous()
+        M, D = int(q.shape[0]), int(v.shape[1])
+        gdt = torch.float32 if (q.dtype == torch.float32 and v.dtype == torch.float32) \
+            else torch.float64
+        g = gout.reshape(M, D).to(gdt).contiguous()
+        gq = torch.empty((M, 3), dtype=q.dtype, device=self.device)
+        cen = (ctypes.c_double * 3)(*[float(c) for c in centroid])
+        with torch.cuda.device(self.device):
+            ws = self._workspace(M, N.NIF_MODE_INTERP)
+            summ = N.Summary()
+            N.check(self._lib.nif_query_grad(self._h, _vp(q), _DT[q.dtype], M, cen, _vp(v),
+                                             _DT[v.dtype], D, _vp(g), _DT[gdt], _vp(gq), _vp(ws),
+                                             ws.numel(), _stream_ptr(self.device),
+                                             ctypes.byref(summ)), 'nif_query_grad')
+            self._raise_rows(summ)
+        return gq
+
     def close(self):
         if getattr(self, '_h', None) is not None and self._h.value:
             self._lib.nif_dmesh_destroy(self._h)
