@@ -54,6 +54,9 @@ def parse():
     p.add_argument('--seed', type=int, default=1)
     p.add_argument('--e2e-steps', type=int, default=3)
     p.add_argument('--no-cpu-baseline', action='store_true')
+    p.add_argument('--mode', default='plain', choices=['plain', 'fwdbwd'],
+                   help='plain: the interpolate workload above; fwdbwd: the differentiable '
+                        'workload (200k keys, 1M queries in [0.1,0.9]^3, D=16, seed 3)')
     return p.parse_args()
 
 
@@ -228,6 +231,58 @@ def cpu_baseline(interp, queries, values):
                           sample, nthreads, sec)}
 
 
+def run_fwdbwd(args, rank, world, local_rank):
+    """Differentiable workload: loss = sum(out * g), backward into queries and values."""
+    import torch
+    import natinterp3d_b200 as ni
+    from natinterp3d_b200 import autograd as nag
+    keys_n = 200_000 if args.keys == 1_000_000 else args.keys
+    q_n = 1_000_000 if args.queries == 10_000_000 else args.queries
+    dim = 16 if args.dim == 3 else args.dim
+    torch.cuda.set_device(local_rank)
+    dev = torch.device('cuda', local_rank)
+    rng = np.random.default_rng([3, rank])
+    keys = rng.uniform(0, 1, (keys_n, 3))
+    interp = ni.Interpolator(keys, device=dev)
+    qd = torch.from_numpy(rng.uniform(0.1, 0.9, (q_n, 3))).to(dev)
+    vd = torch.from_numpy(rng.standard_normal((keys_n, dim)).astype(np.float32)).to(dev)
+    gd = torch.from_numpy(rng.standard_normal((q_n, dim))).to(dev)
+
+    def fwd():
+        return interp.interpolate_device(qd, vd, check=False)
+
+    def fwdbwd():
+        q = qd.clone().requires_grad_(True)
+        v = vd.clone().requires_grad_(True)
+        out = nag.interpolate(interp, q, v)
+        (out * gd).sum().backward()
+        return q.grad, v.grad
+
+    def timed(fn):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / args.steps
+
+    ms_fwd = timed(fwd)
+    ms_fb = timed(fwdbwd)
+    if rank == 0:
+        print(json.dumps({
+            'metric': METRIC, 'mode': 'fwd+bwd', 'value': q_n / (ms_fb * 1e-3), 'unit': 'queries/s',
+            'n_gpus': world, 'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': ms_fb,
+            'plain_forward_ms': ms_fwd, 'fwdbwd_over_forward': ms_fb / ms_fwd,
+            'higher_is_better': True, 'dtype': 'f64', 'data': 'synthetic',
+            'config': {'workload': 'differentiable: %d keys U[0,1]^3, %d queries U[0.1,0.9]^3 float64 '
+                                   'with grad, values D=%d float32 with grad, loss=sum(out*g), seed 3'
+                                   % (keys_n, q_n, dim)}}))
+
+
 def main():
     args = parse()
     rank = int(os.environ.get('RANK', '0'))
@@ -236,6 +291,9 @@ def main():
 
     if args.impl == 'reference':
         run_reference(args, rank, world)
+        return
+    if args.mode == 'fwdbwd':
+        run_fwdbwd(args, rank, world, local_rank)
         return
 
     import torch

@@ -143,11 +143,13 @@ int nif_weights_count(const nif_dmesh *m, const void *d_queries, int query_dtype
 
 /* Sibson weights, step 2 of 2: copies the rows staged by nif_weights_count
  * into CSR arrays d_vals (vals_dtype, nnz) and d_cols (int32, nnz).  Columns
- * of a row appear in natinterp3d's first-seen order.  Replaces the CSR copy
+ * of a row appear in natinterp3d's first-seen order.  If d_row_totals is not
+ * NULL it receives each row's normaliser (the sum of its stolen volumes, 0
+ * for empty rows; float64 [M]), which nif_query_grad takes as input.  Replaces the CSR copy
  * of natural_insertionfree.c:915-928 (natinterp3d mallocs vals/cols itself). */
 int nif_weights_fill(const nif_dmesh *m, int64_t M, const void *d_ws, size_t ws_bytes,
                      const int32_t *d_rowptr, void *d_vals, int vals_dtype, int32_t *d_cols,
-                     void *stream);
+                     double *d_row_totals, void *stream);
 
 /* Interpolation without materialising the weights: out[i, :] =
  * sum_k w_ik values[k, :] for every query, accumulated in row order exactly
@@ -182,12 +184,16 @@ int nif_spmm_t(int64_t M, int64_t N, int64_t nnz, const int32_t *d_rowptr, const
 /* Gradient of a loss through interpolation with respect to the query
  * positions: gq[i, :] = sum_k (gout[i, :] . values[k, :]) dw_ik/dq_i, from the
  * analytic derivative of every stolen volume (the virtual-tet terms of
- * natural_insertionfree.c:681-719; all other terms are locally constant),
- * recomputing each query's cavity.  gout_dtype = promote(query, values);
- * gq has the query dtype; rows without a derivative (empty, or exactly on a
- * data site) get zero.  Workspace: nif_query_workspace_bytes(NIF_MODE_INTERP). */
+ * natural_insertionfree.c:681-719; all other terms are locally constant).
+ * Takes the forward pass's CSR (d_rowptr, float64 d_weights) and row
+ * normalisers (nif_weights_fill's d_row_totals) and recomputes each query's
+ * cavity, boundary and neighbour order instead of storing them.
+ * gout_dtype = promote(query, values); gq has the query dtype; rows without
+ * a derivative (empty, or exactly on a data site) get zero.
+ * Workspace: nif_query_workspace_bytes(NIF_MODE_INTERP). */
 int nif_query_grad(const nif_dmesh *m, const void *d_queries, int query_dtype, int64_t M,
-                   const double centroid[3], const void *d_values, int values_dtype, int D,
+                   const double centroid[3], const int32_t *d_rowptr, const double *d_weights,
+                   const double *d_row_totals, const void *d_values, int values_dtype, int D,
                    const void *d_gout, int gout_dtype, void *d_gq, void *d_ws, size_t ws_bytes,
                    void *stream, nif_summary *summary);
 

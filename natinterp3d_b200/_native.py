@@ -175,7 +175,7 @@ CUDA_SIGNATURES = {
     'nif_weights_count': (c_int, [c_void_p, c_void_p, c_int, c_int64, c_double_p, c_void_p,
                                   c_size_t, c_void_p, c_void_p, ctypes.POINTER(Summary)]),
     'nif_weights_fill': (c_int, [c_void_p, c_int64, c_void_p, c_size_t, c_void_p, c_void_p, c_int,
-                                 c_void_p, c_void_p]),
+                                 c_void_p, c_void_p, c_void_p]),
     'nif_interpolate': (c_int, [c_void_p, c_void_p, c_int, c_int64, c_double_p, c_void_p, c_int,
                                 c_int, c_void_p, c_int, c_void_p, c_size_t, c_void_p,
                                 ctypes.POINTER(Summary)]),
@@ -187,9 +187,9 @@ CUDA_SIGNATURES = {
     'nif_spmm_t_workspace_bytes': (c_int, [c_int64, c_int64, c_int64, ctypes.POINTER(c_size_t)]),
     'nif_spmm_t': (c_int, [c_int64, c_int64, c_int64, c_void_p, c_void_p, c_void_p, c_int, c_void_p,
                            c_int, c_int, c_void_p, c_int, c_void_p, c_size_t, c_void_p]),
-    'nif_query_grad': (c_int, [c_void_p, c_void_p, c_int, c_int64, c_double_p, c_void_p, c_int, c_int,
-                               c_void_p, c_int, c_void_p, c_void_p, c_size_t, c_void_p,
-                               ctypes.POINTER(Summary)]),
+    'nif_query_grad': (c_int, [c_void_p, c_void_p, c_int, c_int64, c_double_p, c_void_p, c_void_p,
+                               c_void_p, c_void_p, c_int, c_int, c_void_p, c_int, c_void_p,
+                               c_void_p, c_size_t, c_void_p, ctypes.POINTER(Summary)]),
     'nif_interpolate_noalloc': (c_int, [c_void_p, c_void_p, c_int, c_int64, c_double_p, c_void_p,
                                         c_int, c_int, c_void_p, c_int, c_void_p,
                                         ctypes.POINTER(Summary)]),

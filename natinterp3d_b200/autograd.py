@@ -30,24 +30,25 @@ class _SibsonFn(torch.autograd.Function):
         dm = interp.device_mesh
         q = queries.detach().contiguous()
         v = values.detach()
-        rowptr, cols, vals = dm.weights_csr(q, interp.centroid, vals_dtype=torch.float64)
+        rowptr, cols, w64, totals = dm.weights_csr(q, interp.centroid, vals_dtype=torch.float64,
+                                                   return_totals=True)
         # weights take the query dtype (as get_weights does); the product uses
         # the promoted dtype of (weights, values), summed in stored column order
-        vals = vals.to(q.dtype)
+        vals = w64.to(q.dtype)
         out = dm.spmm(rowptr, cols, vals, v)
         ctx.interp = interp
         ctx.value_shape = values.shape
-        ctx.save_for_backward(q, v, rowptr, cols, vals)
+        ctx.save_for_backward(q, v, rowptr, cols, vals, w64, totals)
         return out.reshape((q.shape[0],) + tuple(values.shape[1:]))
 
     @staticmethod
     def backward(ctx, grad_out):
-        q, v, rowptr, cols, vals = ctx.saved_tensors
+        q, v, rowptr, cols, vals, w64, totals = ctx.saved_tensors
         dm = ctx.interp.device_mesh
         g = grad_out.contiguous()
         gq = gv = None
         if ctx.needs_input_grad[0]:
-            gq = dm.query_grad(q, v, g, ctx.interp.centroid)
+            gq = dm.query_grad(q, v, g, ctx.interp.centroid, rowptr, w64, totals)
         if ctx.needs_input_grad[1]:
             gv = dm.spmm_t(rowptr, cols, vals, g.reshape(q.shape[0], -1), dm.n_keys)
             gv = gv.reshape(ctx.value_shape).to(v.dtype)

@@ -341,6 +341,8 @@ __global__ void k_scan_apply(const int *__restrict__ in, int64_t n, const OutT *
 
 // get_weights: rows staged per original row index, compacted afterwards
 struct StageSink {
+    static constexpr bool FULL = true;
+    static constexpr int MIN_BLOCKS = NIF_FAST_MINB;
     int *__restrict__ cnt;          // [M]
     int64_t *__restrict__ src;      // [M] first staged entry of the row
     int *__restrict__ cols;         // [M*ROW_CAP + arena]
@@ -348,10 +350,12 @@ struct StageSink {
     int64_t arena_base;             // = M*ROW_CAP
     int64_t arena_cap;
     DevSummary *sum;
+    double *__restrict__ total;     // [M] normaliser of each row (0 for empty rows)
 
     template <int G, class W>
     __device__ __forceinline__ void emit(int64_t i, int nnb, W &ws, const Grp<G> &g, bool large,
-                                         const MeshView &, dv3, const RowInfo &) {
+                                         const MeshView &, dv3, const RowInfo &r) {
+        if (g.lane == 0) total[i] = (nnb > 0) ? r.total : 0.0;
         int64_t o = i * ROW_CAP;
         if (large) {
             unsigned long long a = 0;
@@ -405,6 +409,8 @@ struct InterpSink {
     const VT *__restrict__ values;  // [N][D]
     CT *__restrict__ out;           // [M][D]
     int D;
+    static constexpr bool FULL = true;
+    static constexpr int MIN_BLOCKS = NIF_FAST_MINB;
     static constexpr bool SORTED = sizeof(WT) == 4;
 
     template <int G, class W>
@@ -455,39 +461,53 @@ struct InterpSink {
 };
 
 // d loss / d query: gq[i, :] = sum_k dL/dw_ik dw_ik/dq_i with dL/dw_ik =
-// gout[i, :] . values[k, :] (derivation in nif_grad.cuh).  Rows without a
-// well-defined derivative (empty, outside the super-simplex, or exactly on
-// a data site, where Sibson coordinates are only continuous) get zero.
+// gout[i, :] . values[k, :] (derivation in nif_grad.cuh).  The forward pass's
+// CSR weights and row normalisers are inputs; the kernel rebuilds only each
+// row's cavity, boundary and neighbour order (whose column order matches the
+// CSR row) and differentiates the virtual-tet volumes, one boundary face per
+// lane.  Rows without a derivative (empty, outside the super-simplex, or
+// exactly on a data site, where Sibson coordinates are only continuous) get
+// zero.
 template <class QT, class VT, class GT>
 struct GradSink {
-    const VT *__restrict__ values;  // [N][D]
-    const GT *__restrict__ gout;    // [M][D]
-    QT *__restrict__ gq;            // [M][3]
+    static constexpr bool FULL = false;
+    // the dual-number face gradient holds many FP64 values: fewer, larger threads
+#ifndef NIF_GRAD_MINB
+#define NIF_GRAD_MINB 4
+#endif
+    static constexpr int MIN_BLOCKS = NIF_GRAD_MINB;
+    const VT *__restrict__ values;   // [N][D]
+    const GT *__restrict__ gout;     // [M][D]
+    const int32_t *__restrict__ rowptr;
+    const double *__restrict__ w;    // CSR weights (float64) of the forward pass
+    const double *__restrict__ total;// [M] row normalisers of the forward pass
+    QT *__restrict__ gq;             // [M][3]
     int D;
 
     template <int G, class W>
     __device__ __forceinline__ void emit(int64_t i, int nnb, W &ws, const Grp<G> &g, bool,
                                          const MeshView &M, dv3 q, const RowInfo &r) {
         double gx = 0.0, gy = 0.0, gz = 0.0;
-        if (nnb > 0 && !r.coincident && r.total > 0.0) {
-            double *gk = reinterpret_cast<double *>(&ws.u);  // free after the cavity search
+        const int64_t r0 = rowptr[i];
+        const double S = total[i];
+        if (nnb > 0 && !r.coincident && S > 1e-30 && rowptr[i + 1] - r0 == nnb) {
+            double *ck = reinterpret_cast<double *>(&ws.u);  // free after the cavity search
             const GT *go = gout + i * (int64_t)D;
             for (int s = g.lane; s < nnb; s += G) {
                 const VT *vr = values + (int64_t)ws.nbr_vid[s] * D;
                 double a = 0.0;
                 for (int d = 0; d < D; d++) a += (double)go[d] * (double)vr[d];
-                gk[s] = a;
+                ck[s] = a;
             }
             g.sync();
             double gbar = 0.0;
             if (g.lane == 0)
-                for (int s = 0; s < nnb; s++) gbar += gk[s] * ws.acc[s];
+                for (int s = 0; s < nnb; s++) gbar += ck[s] * w[r0 + s];
             gbar = g.shfl(gbar, 0);
-            const double inv_total = 1.0 / r.total;
-            for (int s = g.lane; s < nnb; s += G) gk[s] = (gk[s] - gbar) * inv_total;
+            const double inv_total = 1.0 / S;
+            for (int s = g.lane; s < nnb; s += G) ck[s] = (ck[s] - gbar) * inv_total;
             g.sync();
-            for (int k = g.lane; k < 3 * r.nbf; k += G) {
-                const int b = k / 3, j = k - 3 * b;
+            for (int b = g.lane; b < r.nbf; b += G) {
                 const int cf = ws.bface[b];
                 const int f = cf & 3;
                 const int tt = ws.cav_tet[cf >> 2];
@@ -495,17 +515,19 @@ struct GradSink {
                 const int va = comp(p, face_vslot(f, 0));
                 const int vb = comp(p, face_vslot(f, 1));
                 const int vc = comp(p, face_vslot(f, 2));
-                const int v = (j == 0) ? va : (j == 1 ? vb : vc);
-                if (v >= M.n) continue;
-                const int s = neighbour_slot(ws, v);
-                if (s < 0) continue;
-                const dv3 dvol = virtual_term_grad(q, vload(M, va), vload(M, vb), vload(M, vc),
-                                                   cload(&M.fcc[4 * (size_t)tt + (3 - f)]), j);
-                // virtual terms enter the stolen volume with a minus sign
-                const double c = gk[s];
-                gx -= c * dvol.x;
-                gy -= c * dvol.y;
-                gz -= c * dvol.z;
+                const int sa = va < M.n ? neighbour_slot(ws, va) : -1;
+                const int sb = vb < M.n ? neighbour_slot(ws, vb) : -1;
+                const int sc = vc < M.n ? neighbour_slot(ws, vc) : -1;
+                // virtual terms enter the stolen volumes with a minus sign
+                const double c0 = sa >= 0 ? -ck[sa] : 0.0;
+                const double c1 = sb >= 0 ? -ck[sb] : 0.0;
+                const double c2 = sc >= 0 ? -ck[sc] : 0.0;
+                if (c0 == 0.0 && c1 == 0.0 && c2 == 0.0) continue;
+                const dv3 gf = virtual_face_grad(q, vload(M, va), vload(M, vb), vload(M, vc),
+                                                 cload(&M.fcc[4 * (size_t)tt + (3 - f)]), c0, c1, c2);
+                gx += gf.x;
+                gy += gf.y;
+                gz += gf.z;
             }
 #pragma unroll
             for (int o = G / 2; o > 0; o >>= 1) {
@@ -701,7 +723,7 @@ __device__ __forceinline__ void record(DevSummary *sum, const RowInfo &r, int la
 
 // fast path: shared-memory scratch, rows in bucket order
 template <class QT, class Sink>
-__global__ void __launch_bounds__(FAST_BLOCK, NIF_FAST_MINB) k_rows_fast(MeshView M, const QT *__restrict__ Q,
+__global__ void __launch_bounds__(FAST_BLOCK, Sink::MIN_BLOCKS) k_rows_fast(MeshView M, const QT *__restrict__ Q,
                                                           Centroid cen, const int *__restrict__ order,
                                                           int64_t nrows, Sink sink, LargeQueue lq,
                                                           DevSummary *sum) {
@@ -716,7 +738,7 @@ __global__ void __launch_bounds__(FAST_BLOCK, NIF_FAST_MINB) k_rows_fast(MeshVie
     for (int64_t s = gid; s < nrows; s += ng) {
         const int64_t i = order[s];
         const dv3 q = load_query(Q, i, cen.c);
-        const RowInfo r = sibson_row<G>(M, q, ws, g);
+        const RowInfo r = sibson_row<G, typename std::remove_reference<decltype(ws)>::type, Sink::FULL>(M, q, ws, g);
         steps += r.steps;
         if (r.status == ST_CAPACITY) {
             if (g.lane == 0) {
@@ -749,7 +771,7 @@ __global__ void __launch_bounds__(32) k_rows_large(MeshView M, const QT *__restr
     for (int j = blockIdx.x; j < nq; j += gridDim.x) {
         const int64_t i = lq.list[j];
         const dv3 q = load_query(Q, i, cen.c);
-        const RowInfo r = sibson_row<G>(M, q, ws, g);
+        const RowInfo r = sibson_row<G, typename std::remove_reference<decltype(ws)>::type, Sink::FULL>(M, q, ws, g);
         steps += r.steps;
         if (g.lane == 0) atomicAdd(&sum->rows_large, 1ull);
         if (r.status != ST_OK) {
@@ -906,6 +928,7 @@ struct QueryLayout {
     int64_t *src, *off64;
     int *scols;
     double *svals;
+    double *rtot;           // per-row normaliser
     int64_t arena_cap;
 };
 
@@ -936,6 +959,7 @@ QueryLayout carve_query(Carve &c, int64_t M, int mode) {
         L.off64 = c.take<int64_t>(M + 1);
         L.scols = c.take<int>(stage);
         L.svals = c.take<double>(stage);
+        L.rtot = c.take<double>(M > 0 ? M : 1);
     }
     return L;
 }
@@ -1230,7 +1254,7 @@ NIF_EXPORT int nif_weights_count(const nif_dmesh *m, const void *d_queries, int 
     Centroid cen{{centroid[0], centroid[1], centroid[2]}};
     NIF_CUDA(cudaMemsetAsync(L.sum, 0, sizeof(DevSummary), st));
     if (M > 0) {
-        StageSink sink{L.cnt, L.src, L.scols, L.svals, M * ROW_CAP, L.arena_cap, L.sum};
+        StageSink sink{L.cnt, L.src, L.scols, L.svals, M * ROW_CAP, L.arena_cap, L.sum, L.rtot};
         if (query_dtype == NIF_F64) {
             run_bucketing(m, static_cast<const double *>(d_queries), M, cen, L, st);
             run_rows(m, static_cast<const double *>(d_queries), M, cen, L, sink, st);
@@ -1252,7 +1276,7 @@ NIF_EXPORT int nif_weights_count(const nif_dmesh *m, const void *d_queries, int 
 
 NIF_EXPORT int nif_weights_fill(const nif_dmesh *m, int64_t M, const void *d_ws, size_t ws_bytes,
                                 const int32_t *d_rowptr, void *d_vals, int vals_dtype,
-                                int32_t *d_cols, void *stream) {
+                                int32_t *d_cols, double *d_row_totals, void *stream) {
     if (!m || M < 0 || M > (int64_t)INT32_MAX || !d_ws || !d_rowptr) return NIF_ERR_ARG;
     if (vals_dtype != NIF_F64 && vals_dtype != NIF_F32) return NIF_ERR_ARG;
     size_t need = 0;
@@ -1264,6 +1288,8 @@ NIF_EXPORT int nif_weights_fill(const nif_dmesh *m, int64_t M, const void *d_ws,
     Carve c{reinterpret_cast<unsigned char *>(const_cast<void *>(d_ws)), 0, ws_bytes, true};
     QueryLayout L = carve_query(c, M, NIF_MODE_WEIGHTS);
     const int blocks = blocks_for(M * 16, 256);
+    if (d_row_totals)
+        NIF_CUDA(cudaMemcpyAsync(d_row_totals, L.rtot, sizeof(double) * M, cudaMemcpyDeviceToDevice, st));
     if (vals_dtype == NIF_F64)
         k_compact<double><<<blocks, 256, 0, st>>>(M, L.cnt, L.src, L.scols, L.svals, d_rowptr, d_cols,
                                                   static_cast<double *>(d_vals));
@@ -1625,24 +1651,27 @@ NIF_EXPORT int nif_spmm_t(int64_t M, int64_t N, int64_t nnz, const int32_t *d_ro
 namespace {
 template <class QT, class VT>
 void grad_typed(const nif_dmesh *m, const void *q, int64_t M, const Centroid &cen, const void *v,
-                int D, const void *gout, void *gq, const QueryLayout &L, cudaStream_t st) {
+                int D, const void *gout, const int32_t *rowptr, const double *w, const double *tot,
+                void *gq, const QueryLayout &L, cudaStream_t st) {
     using GT = typename std::conditional<(sizeof(QT) == 8 || sizeof(VT) == 8), double, float>::type;
-    GradSink<QT, VT, GT> sink{static_cast<const VT *>(v), static_cast<const GT *>(gout),
-                              static_cast<QT *>(gq), D};
+    GradSink<QT, VT, GT> sink{static_cast<const VT *>(v), static_cast<const GT *>(gout), rowptr, w,
+                              tot, static_cast<QT *>(gq), D};
     run_bucketing(m, static_cast<const QT *>(q), M, cen, L, st);
     run_rows(m, static_cast<const QT *>(q), M, cen, L, sink, st);
 }
 }  // namespace
 
 NIF_EXPORT int nif_query_grad(const nif_dmesh *m, const void *d_queries, int query_dtype, int64_t M,
-                              const double centroid[3], const void *d_values, int values_dtype,
-                              int D, const void *d_gout, int gout_dtype, void *d_gq, void *d_ws,
-                              size_t ws_bytes, void *stream, nif_summary *summary) {
+                              const double centroid[3], const int32_t *d_rowptr,
+                              const double *d_weights, const double *d_row_totals,
+                              const void *d_values, int values_dtype, int D, const void *d_gout,
+                              int gout_dtype, void *d_gq, void *d_ws, size_t ws_bytes, void *stream,
+                              nif_summary *summary) {
     int rc = check_query_args(m, d_queries, query_dtype, M, centroid, d_ws);
     if (rc != NIF_OK) return rc;
     if ((values_dtype != NIF_F64 && values_dtype != NIF_F32) || D < 1) return NIF_ERR_ARG;
     if (gout_dtype != expect_promoted(query_dtype, values_dtype)) return NIF_ERR_ARG;
-    if (M > 0 && (!d_values || !d_gout || !d_gq)) return NIF_ERR_ARG;
+    if (M > 0 && (!d_values || !d_gout || !d_gq || !d_rowptr || !d_row_totals)) return NIF_ERR_ARG;
     size_t need = 0;
     nif_query_workspace_bytes(m, M, NIF_MODE_INTERP, &need);
     if (ws_bytes < need) return NIF_ERR_WORKSPACE;
@@ -1653,13 +1682,17 @@ NIF_EXPORT int nif_query_grad(const nif_dmesh *m, const void *d_queries, int que
     NIF_CUDA(cudaMemsetAsync(L.sum, 0, sizeof(DevSummary), st));
     if (M > 0) {
         if (query_dtype == NIF_F64 && values_dtype == NIF_F64)
-            grad_typed<double, double>(m, d_queries, M, cen, d_values, D, d_gout, d_gq, L, st);
+            grad_typed<double, double>(m, d_queries, M, cen, d_values, D, d_gout, d_rowptr, d_weights,
+                                       d_row_totals, d_gq, L, st);
         else if (query_dtype == NIF_F64)
-            grad_typed<double, float>(m, d_queries, M, cen, d_values, D, d_gout, d_gq, L, st);
+            grad_typed<double, float>(m, d_queries, M, cen, d_values, D, d_gout, d_rowptr, d_weights,
+                                       d_row_totals, d_gq, L, st);
         else if (values_dtype == NIF_F32)
-            grad_typed<float, float>(m, d_queries, M, cen, d_values, D, d_gout, d_gq, L, st);
+            grad_typed<float, float>(m, d_queries, M, cen, d_values, D, d_gout, d_rowptr, d_weights,
+                                       d_row_totals, d_gq, L, st);
         else
-            grad_typed<float, double>(m, d_queries, M, cen, d_values, D, d_gout, d_gq, L, st);
+            grad_typed<float, double>(m, d_queries, M, cen, d_values, D, d_gout, d_rowptr, d_weights,
+                                       d_row_totals, d_gq, L, st);
     }
     if (summary) return read_summary(L, st, summary, nullptr);
     return cuda_rc(cudaGetLastError());

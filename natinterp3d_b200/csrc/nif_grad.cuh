@@ -116,18 +116,34 @@ __device__ __forceinline__ dual3 subcell_volume_d(dvec pk, dvec pa, dvec pb, dve
     return vol / dconst(12.0);
 }
 
-// d(virtual-tet term volume)/dq for boundary face (fa, fb, fc), vertex j
-__device__ __forceinline__ dv3 virtual_term_grad(dv3 q, dv3 fa, dv3 fb, dv3 fc, dv3 cface, int j) {
+// Gradient of sum_j c_j * (virtual-tet term of vertex j) over the three
+// vertices of boundary face (fa, fb, fc); c_j = 0 skips a vertex.  The
+// virtual-tet circumcentre and the three (vertex, query, vertex) triangle
+// circumcentres are shared by the face's three terms (each triangle is
+// evaluated in one vertex order; its value part can differ from the other
+// order only in the last bits, which moves no branch of the volume formula).
+__device__ __forceinline__ dv3 virtual_face_grad(dv3 q, dv3 fa, dv3 fb, dv3 fc, dv3 cface, double c0,
+                                                 double c1, double c2) {
     const dvec Q = dvec{dual3{q.x, 1.0, 0.0, 0.0}, dual3{q.y, 0.0, 1.0, 0.0}, dual3{q.z, 0.0, 0.0, 1.0}};
-    const dvec A = dvconst(fa), B = dvconst(fb), C = dvconst(fc);
-    const dvec pk = (j == 0) ? A : (j == 1 ? B : C);
-    const dvec pa = (j == 0) ? B : (j == 1 ? C : A);
-    const dvec pb = (j == 0) ? C : (j == 1 ? A : B);
+    const dvec A = dvconst(fa), B = dvconst(fb), C = dvconst(fc), F = dvconst(cface);
     const dvec ct = tet_cc_d(Q, A, B, C);
-    const dvec f1 = tri_cc_d(pk, Q, pa);
-    const dvec f2 = tri_cc_d(pk, Q, pb);
-    const dual3 vol = subcell_volume_d(pk, Q, pa, pb, ct, f1, f2, dvconst(cface));
-    return dv3{vol.dx, vol.dy, vol.dz};
+    const dvec tab = tri_cc_d(A, Q, B);
+    const dvec tac = tri_cc_d(A, Q, C);
+    const dvec tbc = tri_cc_d(B, Q, C);
+    dv3 gsum = dv3{0.0, 0.0, 0.0};
+    if (c0 != 0.0) {
+        const dual3 v = subcell_volume_d(A, Q, B, C, ct, tab, tac, F);
+        gsum.x += c0 * v.dx; gsum.y += c0 * v.dy; gsum.z += c0 * v.dz;
+    }
+    if (c1 != 0.0) {
+        const dual3 v = subcell_volume_d(B, Q, C, A, ct, tbc, tab, F);
+        gsum.x += c1 * v.dx; gsum.y += c1 * v.dy; gsum.z += c1 * v.dz;
+    }
+    if (c2 != 0.0) {
+        const dual3 v = subcell_volume_d(C, Q, A, B, ct, tac, tbc, F);
+        gsum.x += c2 * v.dx; gsum.y += c2 * v.dy; gsum.z += c2 * v.dz;
+    }
+    return gsum;
 }
 
 }  // namespace nif

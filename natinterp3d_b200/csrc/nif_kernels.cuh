@@ -232,7 +232,10 @@ __device__ __forceinline__ int neighbour_slot(const W &ws, int v) {
 
 // The Sibson row of centred query q.  On ST_OK the row is ws.nbr_vid[0..nnb)
 // with normalised weights ws.acc[0..nnb), in natinterp3d's column order.
-template <int G, class W>
+// With FULL = false only the combinatorial part is built (cavity, visiting
+// order, boundary faces, neighbours in column order) and no volume is
+// computed; the query-gradient kernel needs nothing more.
+template <int G, class W, bool FULL = true>
 __device__ RowInfo sibson_row(const MeshView &M, const dv3 q, W &ws, const Grp<G> &g) {
     using cav_t = typename W::cav_t;
     using slot_t = typename W::slot_t;
@@ -483,6 +486,10 @@ __device__ RowInfo sibson_row(const MeshView &M, const dv3 q, W &ws, const Grp<G
     }
     g.sync();
     if (nnb == 0) return r;
+    if constexpr (!FULL) {
+        r.nnb = nnb;
+        return r;
+    }
 
     // ---- 4. stolen volumes ----------------------------------------------------
     // Items in natinterp3d's order: the 4 vertices of every cavity tet (cavity

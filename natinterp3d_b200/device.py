@@ -82,10 +82,12 @@ class DeviceMesh:
             raise RuntimeError('%d queries exceed the per-query capacity of the large-row kernel '
                                '(cavity larger than 4096 tets)' % summary.rows_failed)
 
-    def weights_csr(self, q, centroid, vals_dtype=torch.float64, return_summary=False):
+    def weights_csr(self, q, centroid, vals_dtype=torch.float64, return_summary=False,
+                    return_totals=False):
         """Sibson weights of device queries q [M, 3] (float32/float64, caller frame).
 
-        Returns (rowptr int32 [M+1], cols int32 [nnz], vals [nnz]) on the device.
+        Returns (rowptr int32 [M+1], cols int32 [nnz], vals [nnz]) on the device,
+        plus the per-row normalisers (float64 [M]) when ``return_totals``.
         """
         _check_device_tensor(q, self.device, 'queries')
         q = q.contiguous()
@@ -109,12 +111,16 @@ class DeviceMesh:
             nnz = int(summ.nnz)
             cols = torch.empty(nnz, dtype=torch.int32, device=self.device)
             vals = torch.empty(nnz, dtype=vals_dtype, device=self.device)
+            totals = torch.empty(M, dtype=torch.float64, device=self.device) if return_totals else None
             N.check(self._lib.nif_weights_fill(self._h, M, _vp(ws), ws.numel(), _vp(rowptr),
-                                               _vp(vals), _DT[vals_dtype], _vp(cols),
+                                               _vp(vals), _DT[vals_dtype], _vp(cols), _vp(totals),
                                                _stream_ptr(self.device)), 'nif_weights_fill')
+        out = (rowptr, cols, vals)
+        if return_totals:
+            out = out + (totals,)
         if return_summary:
-            return rowptr, cols, vals, summ.as_dict()
-        return rowptr, cols, vals
+            out = out + (summ.as_dict(),)
+        return out
 
     def interpolate(self, q, values, centroid, return_summary=False, check=True):
         """out[M, D] = W(q) @ values without materialising W (device tensors)."""
@@ -181,8 +187,9 @@ class DeviceMesh:
                                          _stream_ptr(self.device)), 'nif_spmm_t')
         return y
 
-    def query_grad(self, q, values, gout, centroid):
-        """d loss / d queries for gout = d loss / d interpolate(q, values)."""
+    def query_grad(self, q, values, gout, centroid, rowptr, weights, totals):
+        """d loss / d queries for gout = d loss / d interpolate(q, values), given the
+        forward pass's CSR (rowptr, float64 weights) and row normalisers."""
         q = q.contiguous()
         v = values.reshape(self.n_keys, -1).contiguous()
         M, D = int(q.shape[0]), int(v.shape[1])
@@ -194,10 +201,12 @@ class DeviceMesh:
         with torch.cuda.device(self.device):
             ws = self._workspace(M, N.NIF_MODE_INTERP)
             summ = N.Summary()
-            N.check(self._lib.nif_query_grad(self._h, _vp(q), _DT[q.dtype], M, cen, _vp(v),
-                                             _DT[v.dtype], D, _vp(g), _DT[gdt], _vp(gq), _vp(ws),
-                                             ws.numel(), _stream_ptr(self.device),
-                                             ctypes.byref(summ)), 'nif_query_grad')
+            w64 = weights if weights.dtype == torch.float64 else weights.to(torch.float64)
+            N.check(self._lib.nif_query_grad(self._h, _vp(q), _DT[q.dtype], M, cen, _vp(rowptr),
+                                             _vp(w64), _vp(totals), _vp(v), _DT[v.dtype], D, _vp(g),
+                                             _DT[gdt], _vp(gq), _vp(ws), ws.numel(),
+                                             _stream_ptr(self.device), ctypes.byref(summ)),
+                    'nif_query_grad')
             self._raise_rows(summ)
         return gq
 
