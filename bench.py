@@ -54,9 +54,12 @@ def parse():
     p.add_argument('--seed', type=int, default=1)
     p.add_argument('--e2e-steps', type=int, default=3)
     p.add_argument('--no-cpu-baseline', action='store_true')
-    p.add_argument('--mode', default='plain', choices=['plain', 'fwdbwd'],
+    p.add_argument('--mode', default='plain', choices=['plain', 'fwdbwd', 'batched'],
                    help='plain: the interpolate workload above; fwdbwd: the differentiable '
-                        'workload (200k keys, 1M queries in [0.1,0.9]^3, D=16, seed 3)')
+                        'workload (200k keys, 1M queries in [0.1,0.9]^3, D=16, seed 3); '
+                        'batched: 512 uneven problems (keys log-uniform [500, 100k], queries '
+                        'log-uniform [1k, 200k], boxes of side 0.5-2, D=4 float32, seed 4)')
+    p.add_argument('--problems', type=int, default=512)
     return p.parse_args()
 
 
@@ -283,6 +286,91 @@ def run_fwdbwd(args, rank, world, local_rank):
                                    % (keys_n, q_n, dim)}}))
 
 
+def batched_workload(P, seed):
+    rng = np.random.default_rng(seed)
+    keys, queries = [], []
+    for _ in range(P):
+        nk = int(np.exp(rng.uniform(np.log(500), np.log(100_000))))
+        nq = int(np.exp(rng.uniform(np.log(1_000), np.log(200_000))))
+        lo = rng.uniform(-5, 5, 3)
+        side = rng.uniform(0.5, 2.0, 3)
+        keys.append(lo + side * rng.uniform(0, 1, (nk, 3)))
+        queries.append(lo + side * (0.025 + 0.95 * rng.uniform(0, 1, (nq, 3))))
+    values = [rng.standard_normal((k.shape[0], 4)).astype(np.float32) for k in keys]
+    return keys, queries, values
+
+
+def run_batched(args, rank, world, local_rank):
+    """Uneven batch: one captured graph vs one plain call per problem vs natinterp3d's loop."""
+    import torch
+    from natinterp3d_b200.batch import BatchInterpolator
+    from oracle import oracle
+    torch.cuda.set_device(local_rank)
+    dev = torch.device('cuda', local_rank)
+    keys, queries, values = batched_workload(args.problems, 4 + rank)
+    t0 = time.perf_counter()
+    b = BatchInterpolator(keys, device=dev)
+    build_s = time.perf_counter() - t0
+    qoff = b.query_offsets([len(q) for q in queries])
+    M = int(qoff[-1])
+    qcat = torch.from_numpy(np.concatenate(queries)).to(dev)
+    vcat = torch.from_numpy(np.concatenate(values)).to(dev)
+    graph = b.capture(qcat, qoff, vcat)
+    eager = b.interpolate_per_problem(qcat, qoff, vcat)
+    same = bool(torch.equal(graph.replay(), eager))
+
+    def timed(fn):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / args.steps
+
+    ms_graph = timed(graph.replay)
+    ms_loop = timed(lambda: b.interpolate_per_problem(qcat, qoff, vcat))
+    # host API: one Interpolator.interpolate per problem (numpy in and out) vs one batched call
+    t0 = time.perf_counter()
+    for p in range(args.problems):
+        b.interpolators[p].interpolate(queries[p], values[p])
+    host_loop_s = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    b.interpolate(queries, values)
+    host_batch_s = time.perf_counter() - t0
+    cpu = None
+    if rank == 0 and oracle.ref_available():
+        # natinterp3d's own code, one Interpolator per problem, on a sample of problems
+        nthreads = host_threads()
+        sample = list(range(0, args.problems, max(1, args.problems // 24)))
+        refs = [oracle.RefInterpolator(keys[p], num_threads=nthreads) for p in sample]
+        t0 = time.perf_counter()
+        for r, p in zip(refs, sample):
+            r.interpolate(queries[p], values[p])
+        sec = time.perf_counter() - t0
+        nq = sum(len(queries[p]) for p in sample)
+        cpu = {'value': nq / sec, 'unit': 'queries/s', 'cores': nthreads, 'kind': 'reference',
+               'sample': '%d of %d problems (%d queries): natinterp3d Interpolator per problem, '
+                         'get_weights + scipy W @ values' % (len(sample), args.problems, nq)}
+    if rank == 0:
+        print(json.dumps({
+            'metric': METRIC, 'mode': 'batched', 'value': M / (ms_graph * 1e-3), 'unit': 'queries/s',
+            'n_gpus': world, 'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': ms_graph,
+            'per_problem_launches_ms': ms_loop, 'batched_over_per_problem_speedup': ms_loop / ms_graph,
+            'host_api_per_problem_s': host_loop_s, 'host_api_batched_s': host_batch_s,
+            'host_api_speedup': host_loop_s / host_batch_s,
+            'bit_identical_to_per_problem': same, 'higher_is_better': True, 'dtype': 'f64',
+            'data': 'synthetic', 'cpu_baseline': cpu,
+            'config': {'workload': '%d problems, keys log-uniform [500, 100k] in boxes of side 0.5-2, '
+                                   'queries log-uniform [1k, 200k] in the boxes shrunk 5%%, values D=4 '
+                                   'float32, seed 4' % args.problems,
+                       'total_keys': int(b.n_keys.sum()), 'total_queries': M,
+                       'mesh_build_s': round(build_s, 1)}}))
+
+
 def main():
     args = parse()
     rank = int(os.environ.get('RANK', '0'))
@@ -294,6 +382,9 @@ def main():
         return
     if args.mode == 'fwdbwd':
         run_fwdbwd(args, rank, world, local_rank)
+        return
+    if args.mode == 'batched':
+        run_batched(args, rank, world, local_rank)
         return
 
     import torch

@@ -197,6 +197,36 @@ int nif_query_grad(const nif_dmesh *m, const void *d_queries, int query_dtype, i
                    const void *d_gout, int gout_dtype, void *d_gq, void *d_ws, size_t ws_bytes,
                    void *stream, nif_summary *summary);
 
+/* ---- batched problems (no counterpart in natinterp3d, which needs one
+ * Interpolator and one query call per key set) ------------------------------
+ * A batch groups P resident meshes (each from nif_dmesh_create, all on one
+ * device); d_buf (nif_batch_bytes) receives their device views.  The mesh
+ * handles must outlive the batch. */
+typedef struct nif_dbatch nif_dbatch;
+int nif_batch_bytes(int n_problems, size_t *bytes);
+int nif_batch_create(int n_problems, nif_dmesh *const *meshes, void *d_buf, size_t buf_bytes,
+                     void *stream, nif_dbatch **out);
+void nif_batch_destroy(nif_dbatch *b);
+int nif_batch_workspace_bytes(const nif_dbatch *b, int64_t total_queries, size_t *bytes);
+
+/* Interpolation of every problem at once.  Queries [sum M_p][3] and values
+ * [sum N_p][D] are concatenated by problem; d_query_offsets and
+ * d_key_offsets (int64 [P+1], device) delimit them; d_centroids (float64
+ * [P][3], device) holds each problem's key centroid.  out [sum M_p][D] gets,
+ * per problem, exactly what nif_interpolate returns for that problem alone.
+ * The call makes no host synchronisation and reads nothing from the host,
+ * so a stream capture of it replays as one CUDA graph: bucketing by
+ * (problem, Morton cell), one persistent row kernel whose warps take tiles
+ * of 64 queries from a device work counter, then the large-row kernel.
+ * Read the row counters afterwards with nif_batch_summary. */
+int nif_batch_interpolate(const nif_dbatch *b, const void *d_queries, int query_dtype,
+                          const int64_t *d_query_offsets, const double *d_centroids,
+                          const void *d_values, int values_dtype, const int64_t *d_key_offsets, int D,
+                          void *d_out, int out_dtype, int64_t total_queries, void *d_ws,
+                          size_t ws_bytes, void *stream);
+int nif_batch_summary(const nif_dbatch *b, int64_t total_queries, const void *d_ws, size_t ws_bytes,
+                      void *stream, nif_summary *summary);
+
 /* Measurement.  While enabled, every query call records CUDA events on its
  * stream between its phases; nif_profile_read waits for the last call's
  * final event and returns the device time in milliseconds of

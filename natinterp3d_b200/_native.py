@@ -190,6 +190,16 @@ CUDA_SIGNATURES = {
     'nif_query_grad': (c_int, [c_void_p, c_void_p, c_int, c_int64, c_double_p, c_void_p, c_void_p,
                                c_void_p, c_void_p, c_int, c_int, c_void_p, c_int, c_void_p,
                                c_void_p, c_size_t, c_void_p, ctypes.POINTER(Summary)]),
+    'nif_batch_bytes': (c_int, [c_int, ctypes.POINTER(c_size_t)]),
+    'nif_batch_create': (c_int, [c_int, ctypes.POINTER(c_void_p), c_void_p, c_size_t, c_void_p,
+                                 ctypes.POINTER(c_void_p)]),
+    'nif_batch_destroy': (None, [c_void_p]),
+    'nif_batch_workspace_bytes': (c_int, [c_void_p, c_int64, ctypes.POINTER(c_size_t)]),
+    'nif_batch_interpolate': (c_int, [c_void_p, c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_int,
+                                      c_void_p, c_int, c_void_p, c_int, c_int64, c_void_p, c_size_t,
+                                      c_void_p]),
+    'nif_batch_summary': (c_int, [c_void_p, c_int64, c_void_p, c_size_t, c_void_p,
+                                  ctypes.POINTER(Summary)]),
     'nif_interpolate_noalloc': (c_int, [c_void_p, c_void_p, c_int, c_int64, c_double_p, c_void_p,
                                         c_int, c_int, c_void_p, c_int, c_void_p,
                                         ctypes.POINTER(Summary)]),

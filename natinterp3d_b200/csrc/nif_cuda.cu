@@ -1697,3 +1697,369 @@ NIF_EXPORT int nif_query_grad(const nif_dmesh *m, const void *d_queries, int que
     if (summary) return read_summary(L, st, summary, nullptr);
     return cuda_rc(cudaGetLastError());
 }
+
+// ===========================================================================
+// Batched interpolation: many independent (keys, queries) problems in one
+// pipeline with no host synchronisation, so that it can be captured in a
+// CUDA graph.  Every problem keeps its own resident mesh (nif_dmesh_create);
+// the batch holds the device array of their views.  Queries, centroids,
+// values and outputs are concatenated by problem, with int64 offsets.
+// ===========================================================================
+namespace nif {
+
+constexpr int BATCH_TILE = 64;  // queries per work item of the persistent kernel
+
+__device__ __forceinline__ int find_problem(const int64_t *__restrict__ off, int P, int64_t i) {
+    int lo = 0, hi = P;  // off[lo] <= i < off[hi]
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (off[mid] <= i) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ int bucket_bits_dev(int64_t M) {
+    int b = 1;
+    while (b < 10 && ((int64_t)1 << (3 * (b + 1))) <= M / 2) b++;
+    return b;
+}
+
+// per-problem bucket bases (one thread; P is small)
+__global__ void k_batch_setup(const int64_t *__restrict__ qoff, int P, int *__restrict__ bits,
+                              int64_t *__restrict__ bbase) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    int64_t acc = 0;
+    for (int p = 0; p < P; p++) {
+        const int b = bucket_bits_dev(qoff[p + 1] - qoff[p]);
+        bits[p] = b;
+        bbase[p] = acc;
+        acc += (int64_t)1 << (3 * b);
+    }
+    bbase[P] = acc;
+}
+
+template <class QT>
+__global__ void k_batch_bucket(const QT *__restrict__ Q, int64_t M, const int64_t *__restrict__ qoff,
+                               int P, const double *__restrict__ cens, const MeshView *__restrict__ views,
+                               const int *__restrict__ bits, const int64_t *__restrict__ bbase,
+                               int *__restrict__ bucket, int *__restrict__ bcount) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < M;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const int p = find_problem(qoff, P, i);
+        const dv3 q = load_query(Q, i, cens + 3 * p);
+        const MeshView &mv = views[p];
+        const int b = bits[p];
+        const double scale = (double)(1 << b);
+        const double c[3] = {q.x, q.y, q.z};
+        unsigned code = 0;
+        for (int a = 0; a < 3; a++) {
+            const double f = (c[a] - mv.glo[a]) * mv.ginv[a] / (double)mv.gdim[a] * scale;
+            const int k = (f >= 0.0) ? (f < scale ? (int)f : (1 << b) - 1) : 0;
+            code |= spread3((unsigned)k) << a;
+        }
+        const int64_t bk = bbase[p] + code;
+        bucket[i] = (int)bk;
+        atomicAdd(&bcount[bk], 1);
+    }
+}
+
+// interpolation sink of a batch: values and outputs of query i belong to its problem
+template <class WT, class VT, class CT>
+struct BatchInterpSink {
+    static constexpr bool FULL = true;
+    static constexpr int MIN_BLOCKS = NIF_FAST_MINB;
+    const VT *__restrict__ values;   // concatenated [sum N_p][D]
+    const int64_t *__restrict__ koff; // [P+1] key offsets
+    const int64_t *__restrict__ qoff; // [P+1] query offsets
+    int P;
+    CT *__restrict__ out;             // concatenated [sum M_p][D]
+    int D;
+
+    template <int G, class W>
+    __device__ __forceinline__ void emit(int64_t i, int nnb, W &ws, const Grp<G> &g, bool large,
+                                         const MeshView &M, dv3 q, const RowInfo &r) {
+        const int p = find_problem(qoff, P, i);
+        InterpSink<WT, VT, CT> s{values + koff[p] * D, out, D};
+        s.template emit<G>(i, nnb, ws, g, large, M, q, r);
+    }
+};
+
+// persistent row kernel of a batch: warps pull tiles of bucket-ordered
+// queries from a device counter; the mesh view of the current problem is
+// kept in shared memory
+template <class QT, class Sink>
+__global__ void __launch_bounds__(FAST_BLOCK, Sink::MIN_BLOCKS)
+    k_rows_batch(const MeshView *__restrict__ views, const int64_t *__restrict__ qoff, int P,
+                 const QT *__restrict__ Q, const double *__restrict__ cens,
+                 const int *__restrict__ order, int64_t nrows, Sink sink, LargeQueue lq,
+                 DevSummary *sum, unsigned long long *counter) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    constexpr int G = FAST_G;
+    constexpr int GPB = FAST_BLOCK / G;
+    __shared__ MeshView sview[GPB];
+    Grp<G> g;
+    const int gib = threadIdx.x / G;
+    FastWS &ws = reinterpret_cast<FastWS *>(smem)[gib];
+    MeshView &M = sview[gib];
+    int cur = -1;
+    unsigned long long steps = 0;
+    for (;;) {
+        unsigned long long tile = 0;
+        if (g.lane == 0) tile = atomicAdd(counter, 1ull);
+        tile = __shfl_sync(g.mask, tile, 0, G);
+        const int64_t s0 = (int64_t)tile * BATCH_TILE;
+        if (s0 >= nrows) break;
+        const int64_t s1 = min(nrows, s0 + BATCH_TILE);
+        for (int64_t s = s0; s < s1; s++) {
+            const int64_t i = order[s];
+            const int p = find_problem(qoff, P, i);
+            if (p != cur) {
+                g.sync();
+                if (g.lane == 0) M = views[p];
+                g.sync();
+                cur = p;
+            }
+            const dv3 q = load_query(Q, i, cens + 3 * p);
+            const RowInfo r = sibson_row<G, FastWS, Sink::FULL>(M, q, ws, g);
+            steps += r.steps;
+            if (r.status == ST_CAPACITY) {
+                if (g.lane == 0) {
+                    const int slot = atomicAdd(&sum->large_count, 1);
+                    lq.list[slot] = (int)i;
+                }
+            } else {
+                if (r.status != ST_OK && g.lane == 0) {
+                    atomicAdd(&sum->rows_failed, 1ull);
+                    atomicCAS(&sum->first_status, 0, NIF_ERR_WALK);
+                }
+                if (r.outside && g.lane == 0) atomicAdd(&sum->rows_outside, 1ull);
+                sink.template emit<G>(i, r.status == ST_OK ? r.nnb : 0, ws, g, false, M, q, r);
+            }
+            g.sync();
+        }
+    }
+    if (g.lane == 0 && steps) atomicAdd(&sum->walk_steps, steps);
+}
+
+template <class QT, class Sink>
+__global__ void __launch_bounds__(32) k_rows_batch_large(const MeshView *__restrict__ views,
+                                                         const int64_t *__restrict__ qoff, int P,
+                                                         const QT *__restrict__ Q,
+                                                         const double *__restrict__ cens, LargeQueue lq,
+                                                         Sink sink, LargeWS *__restrict__ wsv,
+                                                         DevSummary *sum) {
+    constexpr int G = LARGE_G;
+    __shared__ MeshView M;
+    Grp<G> g;
+    LargeWS &ws = wsv[blockIdx.x];
+    const int nq = sum->large_count;
+    int cur = -1;
+    for (int j = blockIdx.x; j < nq; j += gridDim.x) {
+        const int64_t i = lq.list[j];
+        const int p = find_problem(qoff, P, i);
+        if (p != cur) {
+            g.sync();
+            if (g.lane == 0) M = views[p];
+            g.sync();
+            cur = p;
+        }
+        const dv3 q = load_query(Q, i, cens + 3 * p);
+        const RowInfo r = sibson_row<G, LargeWS, Sink::FULL>(M, q, ws, g);
+        if (g.lane == 0) atomicAdd(&sum->rows_large, 1ull);
+        if (r.status != ST_OK) {
+            if (g.lane == 0) {
+                atomicAdd(&sum->rows_failed, 1ull);
+                atomicCAS(&sum->first_status, 0, r.status == ST_WALK ? NIF_ERR_WALK : NIF_ERR_CAPACITY);
+            }
+            sink.template emit<G>(i, 0, ws, g, true, M, q, r);
+        } else {
+            sink.template emit<G>(i, r.nnb, ws, g, true, M, q, r);
+        }
+        g.sync();
+    }
+}
+
+}  // namespace nif
+
+struct nif_dbatch {
+    int P;
+    int device;
+    int num_sms;
+    MeshView *d_views;  // [P] in the caller's buffer
+};
+
+namespace {
+
+struct BatchLayout {
+    DevSummary *sum;
+    unsigned long long *counter;
+    int *bits, *bucket, *bcount, *order, *large_list, *bsum, *btotal;
+    int64_t *bbase;
+    LargeWS *large_ws;
+};
+
+BatchLayout carve_batch(Carve &c, int P, int64_t M) {
+    BatchLayout L{};
+    const int64_t nbk = 8 * (int64_t)P + M / 2 + 1;
+    L.sum = c.take<DevSummary>(1);
+    L.counter = c.take<unsigned long long>(1);
+    L.bits = c.take<int>(P);
+    L.bbase = c.take<int64_t>(P + 1);
+    L.bucket = c.take<int>(M > 0 ? M : 1);
+    L.bcount = c.take<int>(nbk + 1);
+    L.order = c.take<int>(M > 0 ? M : 1);
+    L.large_list = c.take<int>(M > 0 ? M : 1);
+    L.bsum = c.take<int>((nbk + 1 + SCAN_TILE - 1) / SCAN_TILE + 1);
+    L.btotal = c.take<int>(2);
+    L.large_ws = c.take<LargeWS>(LARGE_GROUPS);
+    return L;
+}
+
+template <class QT, class VT, class CT>
+void batch_typed(const nif_dbatch *b, const void *q, int64_t M, const int64_t *qoff, const double *cens,
+                 const void *v, const int64_t *koff, int D, void *out, const BatchLayout &L,
+                 cudaStream_t st) {
+    using Sink = BatchInterpSink<QT, VT, CT>;
+    const QT *Q = static_cast<const QT *>(q);
+    const int64_t nbk = 8 * (int64_t)b->P + M / 2 + 1;
+    cudaMemsetAsync(L.sum, 0, sizeof(DevSummary), st);
+    cudaMemsetAsync(L.counter, 0, sizeof(unsigned long long), st);
+    cudaMemsetAsync(L.bcount, 0, sizeof(int) * (nbk + 1), st);
+    k_batch_setup<<<1, 1, 0, st>>>(qoff, b->P, L.bits, L.bbase);
+    k_batch_bucket<QT><<<blocks_for(M, 256), 256, 0, st>>>(Q, M, qoff, b->P, cens, b->d_views, L.bits,
+                                                          L.bbase, L.bucket, L.bcount);
+    launch_scan<int>(L.bcount, nbk, L.bsum, L.btotal, L.bcount, st);
+    k_scatter<<<blocks_for(M, 256), 256, 0, st>>>(L.bucket, M, L.bcount, L.order);
+    Sink sink{static_cast<const VT *>(v), koff, qoff, b->P, static_cast<CT *>(out), D};
+    constexpr int GPB = FAST_BLOCK / FAST_G;
+    const size_t smem = GPB * sizeof(FastWS);
+    auto kern = k_rows_batch<QT, Sink>;
+    static int per_sm = -1;
+    if (per_sm < 0) {
+        if (smem > 40 * 1024) set_smem(kern, smem);
+        per_sm = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, FAST_BLOCK, smem);
+        if (per_sm < 1) per_sm = 1;
+    }
+    const int64_t want = (M + (int64_t)GPB * BATCH_TILE - 1) / ((int64_t)GPB * BATCH_TILE);
+    int64_t blocks = (int64_t)per_sm * b->num_sms;
+    if (blocks > want) blocks = want;
+    if (blocks < 1) blocks = 1;
+    kern<<<(unsigned)blocks, FAST_BLOCK, smem, st>>>(b->d_views, qoff, b->P, Q, cens, L.order, M, sink,
+                                                    LargeQueue{L.large_list}, L.sum, L.counter);
+    k_rows_batch_large<QT, Sink><<<LARGE_GROUPS, 32, 0, st>>>(b->d_views, qoff, b->P, Q, cens,
+                                                             LargeQueue{L.large_list}, sink,
+                                                             L.large_ws, L.sum);
+}
+
+}  // namespace
+
+NIF_EXPORT int nif_batch_bytes(int n_problems, size_t *bytes) {
+    if (!bytes || n_problems < 1) return NIF_ERR_ARG;
+    *bytes = align_up(sizeof(MeshView) * (size_t)n_problems, 256);
+    return NIF_OK;
+}
+
+NIF_EXPORT int nif_batch_create(int n_problems, nif_dmesh *const *meshes, void *d_buf, size_t buf_bytes,
+                                void *stream, nif_dbatch **out) {
+    if (!out || !meshes || n_problems < 1 || !d_buf) return NIF_ERR_ARG;
+    *out = nullptr;
+    size_t need = 0;
+    nif_batch_bytes(n_problems, &need);
+    if (buf_bytes < need) return NIF_ERR_WORKSPACE;
+    MeshView *host = static_cast<MeshView *>(malloc(sizeof(MeshView) * (size_t)n_problems));
+    if (!host) return NIF_ERR_NOMEM;
+    int dev = -1;
+    for (int p = 0; p < n_problems; p++) {
+        if (!meshes[p] || (p > 0 && meshes[p]->device != dev)) {
+            free(host);
+            return NIF_ERR_ARG;
+        }
+        dev = meshes[p]->device;
+        host[p] = meshes[p]->view;
+    }
+    cudaStream_t st = S(stream);
+    if (cudaMemcpyAsync(d_buf, host, sizeof(MeshView) * (size_t)n_problems, cudaMemcpyHostToDevice, st) !=
+            cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess) {
+        free(host);
+        return NIF_ERR_CUDA;
+    }
+    free(host);
+    nif_dbatch *b = new (std::nothrow) nif_dbatch();
+    if (!b) return NIF_ERR_NOMEM;
+    b->P = n_problems;
+    b->device = dev;
+    b->num_sms = meshes[0]->num_sms;
+    b->d_views = static_cast<MeshView *>(d_buf);
+    *out = b;
+    return NIF_OK;
+}
+
+NIF_EXPORT void nif_batch_destroy(nif_dbatch *b) { delete b; }
+
+NIF_EXPORT int nif_batch_workspace_bytes(const nif_dbatch *b, int64_t total_queries, size_t *bytes) {
+    if (!b || !bytes || total_queries < 0 || total_queries > (int64_t)INT32_MAX) return NIF_ERR_ARG;
+    Carve c{nullptr, 0, (size_t)-1, true};
+    carve_batch(c, b->P, total_queries);
+    *bytes = align_up(c.off, 256);
+    return NIF_OK;
+}
+
+NIF_EXPORT int nif_batch_interpolate(const nif_dbatch *b, const void *d_queries, int query_dtype,
+                                     const int64_t *d_query_offsets, const double *d_centroids,
+                                     const void *d_values, int values_dtype,
+                                     const int64_t *d_key_offsets, int D, void *d_out, int out_dtype,
+                                     int64_t total_queries, void *d_ws, size_t ws_bytes, void *stream) {
+    if (!b || total_queries < 0 || total_queries > (int64_t)INT32_MAX || D < 1) return NIF_ERR_ARG;
+    if ((query_dtype != NIF_F64 && query_dtype != NIF_F32) ||
+        (values_dtype != NIF_F64 && values_dtype != NIF_F32))
+        return NIF_ERR_ARG;
+    if (out_dtype != expect_promoted(query_dtype, values_dtype)) return NIF_ERR_ARG;
+    if (!d_query_offsets || !d_centroids || !d_key_offsets || !d_ws) return NIF_ERR_ARG;
+    if (total_queries > 0 && (!d_queries || !d_values || !d_out)) return NIF_ERR_ARG;
+    if (reinterpret_cast<uintptr_t>(d_ws) % 256 != 0) return NIF_ERR_ARG;
+    size_t need = 0;
+    nif_batch_workspace_bytes(b, total_queries, &need);
+    if (ws_bytes < need) return NIF_ERR_WORKSPACE;
+    cudaStream_t st = S(stream);
+    Carve c{reinterpret_cast<unsigned char *>(d_ws), 0, ws_bytes, true};
+    BatchLayout L = carve_batch(c, b->P, total_queries);
+    if (total_queries == 0) return cuda_rc(cudaMemsetAsync(L.sum, 0, sizeof(DevSummary), st));
+    const int64_t M = total_queries;
+    if (query_dtype == NIF_F64 && values_dtype == NIF_F64)
+        batch_typed<double, double, double>(b, d_queries, M, d_query_offsets, d_centroids, d_values,
+                                            d_key_offsets, D, d_out, L, st);
+    else if (query_dtype == NIF_F64)
+        batch_typed<double, float, double>(b, d_queries, M, d_query_offsets, d_centroids, d_values,
+                                           d_key_offsets, D, d_out, L, st);
+    else if (values_dtype == NIF_F32)
+        batch_typed<float, float, float>(b, d_queries, M, d_query_offsets, d_centroids, d_values,
+                                         d_key_offsets, D, d_out, L, st);
+    else
+        batch_typed<float, double, double>(b, d_queries, M, d_query_offsets, d_centroids, d_values,
+                                           d_key_offsets, D, d_out, L, st);
+    return cuda_rc(cudaGetLastError());
+}
+
+NIF_EXPORT int nif_batch_summary(const nif_dbatch *b, int64_t total_queries, const void *d_ws,
+                                 size_t ws_bytes, void *stream, nif_summary *summary) {
+    if (!b || !summary || !d_ws) return NIF_ERR_ARG;
+    size_t need = 0;
+    if (nif_batch_workspace_bytes(b, total_queries, &need) != NIF_OK || ws_bytes < need)
+        return NIF_ERR_WORKSPACE;
+    Carve c{reinterpret_cast<unsigned char *>(const_cast<void *>(d_ws)), 0, ws_bytes, true};
+    BatchLayout L = carve_batch(c, b->P, total_queries);
+    DevSummary d;
+    cudaStream_t st = S(stream);
+    NIF_CUDA(cudaMemcpyAsync(&d, L.sum, sizeof(d), cudaMemcpyDeviceToHost, st));
+    NIF_CUDA(cudaStreamSynchronize(st));
+    summary->nnz = 0;
+    summary->rows_large = (int64_t)d.rows_large;
+    summary->rows_failed = (int64_t)d.rows_failed;
+    summary->rows_outside = (int64_t)d.rows_outside;
+    summary->walk_steps = (int64_t)d.walk_steps;
+    summary->first_status = d.first_status;
+    summary->reserved = 0;
+    return NIF_OK;
+}
