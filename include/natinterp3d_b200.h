@@ -151,6 +151,12 @@ int nif_weights_fill(const nif_dmesh *m, int64_t M, const void *d_ws, size_t ws_
                      const int32_t *d_rowptr, void *d_vals, int vals_dtype, int32_t *d_cols,
                      double *d_row_totals, void *stream);
 
+/* Row counters of the last nif_interpolate / nif_query_grad call that used
+ * this workspace (for calls made with summary = NULL, which do not
+ * synchronise).  Synchronises `stream`. */
+int nif_query_summary(const nif_dmesh *m, int64_t M, int mode, const void *d_ws, size_t ws_bytes,
+                      void *stream, nif_summary *summary);
+
 /* Interpolation without materialising the weights: out[i, :] =
  * sum_k w_ik values[k, :] for every query, accumulated in row order exactly
  * as `get_weights(Q) @ values` (natinterp3d.py:131-137, scipy csr_matvecs)

@@ -182,6 +182,8 @@ CUDA_SIGNATURES = {
     'nif_profile_enable': (c_int, [c_int]),
     'nif_profile_read': (c_int, [c_double_p]),
     'nif_measure_fp64_peak': (c_int, [c_double_p, c_double_p]),
+    'nif_query_summary': (c_int, [c_void_p, c_int64, c_int, c_void_p, c_size_t, c_void_p,
+                                  ctypes.POINTER(Summary)]),
     'nif_spmm': (c_int, [c_int64, c_int64, c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_int,
                          c_int, c_void_p, c_int, c_void_p]),
     'nif_spmm_t_workspace_bytes': (c_int, [c_int64, c_int64, c_int64, ctypes.POINTER(c_size_t)]),

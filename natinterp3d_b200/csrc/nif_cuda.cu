@@ -2063,3 +2063,15 @@ NIF_EXPORT int nif_batch_summary(const nif_dbatch *b, int64_t total_queries, con
     summary->reserved = 0;
     return NIF_OK;
 }
+
+NIF_EXPORT int nif_query_summary(const nif_dmesh *m, int64_t M, int mode, const void *d_ws,
+                                 size_t ws_bytes, void *stream, nif_summary *summary) {
+    if (!m || !summary || !d_ws || M < 0) return NIF_ERR_ARG;
+    size_t need = 0;
+    int rc = nif_query_workspace_bytes(m, M, mode, &need);
+    if (rc != NIF_OK) return rc;
+    if (ws_bytes < need) return NIF_ERR_WORKSPACE;
+    Carve c{reinterpret_cast<unsigned char *>(const_cast<void *>(d_ws)), 0, ws_bytes, true};
+    QueryLayout L = carve_query(c, M, mode);
+    return read_summary(L, S(stream), summary, nullptr);
+}

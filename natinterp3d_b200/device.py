@@ -20,7 +20,14 @@ def _stream_ptr(device):
 
 
 def _vp(t):
-    return ctypes.c_void_p(t.data_ptr()) if t is not None and t.numel() > 0 else ctypes.c_void_p(0)
+    """Device address of a tensor; a zero-element view of an allocated buffer
+    passes its storage's address (PyTorch reports 0 for empty tensors)."""
+    if t is None:
+        return ctypes.c_void_p(0)
+    if t.numel() > 0:
+        return ctypes.c_void_p(t.data_ptr())
+    st = t.untyped_storage()
+    return ctypes.c_void_p(st.data_ptr() if st.size() > 0 else 0)
 
 
 def _check_device_tensor(t, device, name):
@@ -109,9 +116,11 @@ class DeviceMesh:
             N.check(rc, 'nif_weights_count')
             self._raise_rows(summ)
             nnz = int(summ.nnz)
-            cols = torch.empty(nnz, dtype=torch.int32, device=self.device)
-            vals = torch.empty(nnz, dtype=vals_dtype, device=self.device)
-            totals = torch.empty(M, dtype=torch.float64, device=self.device) if return_totals else None
+            # at least one element each, so the library always gets real pointers
+            cols = torch.empty(max(nnz, 1), dtype=torch.int32, device=self.device)[:nnz]
+            vals = torch.empty(max(nnz, 1), dtype=vals_dtype, device=self.device)[:nnz]
+            totals = torch.empty(max(M, 1), dtype=torch.float64, device=self.device)[:M] \
+                if return_totals else None
             N.check(self._lib.nif_weights_fill(self._h, M, _vp(ws), ws.numel(), _vp(rowptr),
                                                _vp(vals), _DT[vals_dtype], _vp(cols), _vp(totals),
                                                _stream_ptr(self.device)), 'nif_weights_fill')
@@ -122,8 +131,11 @@ class DeviceMesh:
             out = out + (summ.as_dict(),)
         return out
 
-    def interpolate(self, q, values, centroid, return_summary=False, check=True):
-        """out[M, D] = W(q) @ values without materialising W (device tensors)."""
+    def interpolate(self, q, values, centroid, return_summary=False, check=True, sync=True):
+        """out[M, D] = W(q) @ values without materialising W (device tensors).
+
+        With ``sync=False`` and ``return_summary`` the row counters are left on
+        the device (returned as a pending handle for :meth:`raise_pending`)."""
         _check_device_tensor(q, self.device, 'queries')
         _check_device_tensor(values, self.device, 'values')
         q = q.contiguous()
@@ -143,17 +155,30 @@ class DeviceMesh:
             ws = self._workspace(M, N.NIF_MODE_INTERP)
             out = torch.empty((M, D), dtype=out_dtype, device=self.device)
             summ = N.Summary()
+            want = check or (return_summary and sync)
             N.check(self._lib.nif_interpolate(self._h, _vp(q), _DT[q.dtype], M, cen, _vp(v),
                                               _DT[v.dtype], D, _vp(out), _DT[out_dtype], _vp(ws),
                                               ws.numel(), _stream_ptr(self.device),
-                                              ctypes.byref(summ) if check else None),
+                                              ctypes.byref(summ) if want else None),
                     'nif_interpolate')
             if check:
                 self._raise_rows(summ)
         out = out[:, 0] if squeeze else out
         if return_summary:
+            if not sync and not check:
+                return out, (M, ws)   # counters stay on the device
             return out, summ.as_dict()
         return out
+
+    def raise_pending(self, pending):
+        """Read the row counters of interpolate(..., sync=False) calls (after they
+        ran) and raise if any row failed."""
+        for M, ws in pending:
+            summ = N.Summary()
+            N.check(self._lib.nif_query_summary(self._h, int(M), N.NIF_MODE_INTERP, _vp(ws),
+                                                ws.numel(), _stream_ptr(self.device),
+                                                ctypes.byref(summ)), 'nif_query_summary')
+            self._raise_rows(summ)
 
     # -------------------------------------------------------------- sparse / grad
     def spmm(self, rowptr, cols, vals, x):

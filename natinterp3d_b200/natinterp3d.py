@@ -29,6 +29,7 @@ from ._native import HostMesh
 from .device import DeviceMesh
 
 _FLOATS = (np.dtype(np.float32), np.dtype(np.float64))
+PIPELINE_CHUNK = 1 << 21  # queries per chunk of the pipelined host interpolation
 
 
 def interpolate(
@@ -173,10 +174,58 @@ class Interpolator:
             raise ValueError('dimension mismatch')
         q = self._host_queries(query_points)
         dm = self.device_mesh
-        qd = torch.from_numpy(q).to(dm.device)
         vd = torch.from_numpy(np.ascontiguousarray(values)).to(dm.device)
+        if q.shape[0] > 2 * PIPELINE_CHUNK:
+            return self._interpolate_pipelined(q, vd)
+        qd = torch.from_numpy(q).to(dm.device)
         out = dm.interpolate(qd, vd, self._centroid)
         return out.cpu().numpy()
+
+    def _interpolate_pipelined(self, q, vd):
+        """Large host batches in chunks: while the kernels of one chunk run, the
+        next chunk's queries go to the device and the previous chunk's results
+        come back, on a separate copy stream through pinned staging buffers."""
+        dm = self.device_mesh
+        dev = dm.device
+        M = q.shape[0]
+        D = 1 if vd.dim() == 1 else int(vd.shape[1])
+        odt = torch.float32 if (q.dtype == np.float32 and vd.dtype == torch.float32) else torch.float64
+        out = np.empty((M, D), dtype=np.float32 if odt == torch.float32 else np.float64)
+        bounds = [(a, min(M, a + PIPELINE_CHUNK)) for a in range(0, M, PIPELINE_CHUNK)]
+        compute = torch.cuda.current_stream(dev)
+        copy = torch.cuda.Stream(device=dev)
+        staging = [torch.empty((PIPELINE_CHUNK, D), dtype=odt, pin_memory=True) for _ in range(2)]
+        failed = []
+        pending = None  # (slot, rows, device result, event)
+
+        def drain(item):
+            slot, (a, b), res, done = item
+            copy.wait_event(done)
+            with torch.cuda.stream(copy):
+                staging[slot][:b - a].copy_(res.reshape(b - a, D), non_blocking=True)
+                res.record_stream(copy)
+            copy.synchronize()
+            out[a:b] = staging[slot][:b - a].numpy()
+
+        with torch.cuda.device(dev):
+            for k, (a, b) in enumerate(bounds):
+                with torch.cuda.stream(copy):
+                    qd = torch.from_numpy(q[a:b]).to(dev)
+                    loaded = torch.cuda.Event()
+                    loaded.record(copy)
+                compute.wait_event(loaded)
+                qd.record_stream(compute)
+                res, summ = dm.interpolate(qd, vd, self._centroid, return_summary=True,
+                                           check=False, sync=False)
+                failed.append(summ)
+                done = torch.cuda.Event()
+                done.record(compute)
+                if pending is not None:
+                    drain(pending)
+                pending = (k % 2, (a, b), res, done)
+            drain(pending)
+        dm.raise_pending(failed)
+        return out[:, 0] if vd.dim() == 1 else out
 
     # -------------------------------------------------------- device-resident API
     def get_weights_device(self, queries: torch.Tensor, dtype=None, as_torch_csr=False):

@@ -182,3 +182,22 @@ def test_float32_queries_and_values(cuda_device):
     out = I.interpolate(q, v)
     assert out.dtype == np.float32
     assert np.array_equal(out, ref @ v)
+
+
+def test_pipelined_host_interpolate_matches_single_call(cuda_device):
+    # more than two pipeline chunks: the chunked host path must return exactly
+    # what one device-resident call returns
+    from natinterp3d_b200 import natinterp3d as api
+    rng = np.random.default_rng(9)
+    keys = rng.uniform(0, 1, (20000, 3))
+    I = ni.Interpolator(keys)
+    M = 2 * api.PIPELINE_CHUNK + 12345
+    q = rng.uniform(0.0, 1.0, (M, 3))
+    v = rng.normal(size=(20000, 3)).astype(np.float32)
+    out = I.interpolate(q, v)
+    ref = I.interpolate_device(torch.from_numpy(q).to(cuda_device),
+                               torch.from_numpy(v).to(cuda_device)).cpu().numpy()
+    assert out.shape == (M, 3) and out.dtype == np.float64
+    assert np.array_equal(out, ref)
+    out1 = I.interpolate(q, v[:, 0])
+    assert out1.shape == (M,) and np.array_equal(out1, ref[:, 0])
