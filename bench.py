@@ -54,6 +54,9 @@ def parse():
     p.add_argument('--seed', type=int, default=1)
     p.add_argument('--e2e-steps', type=int, default=3)
     p.add_argument('--no-cpu-baseline', action='store_true')
+    p.add_argument('--predicates', default='fast', choices=['fast', 'audit', 'exact'],
+                   help="geometric predicates: natinterp3d's fast signs (default), the same "
+                        "signs with uncertain evaluations counted, or exact signs")
     p.add_argument('--mode', default='plain', choices=['plain', 'fwdbwd', 'batched'],
                    help='plain: the interpolate workload above; fwdbwd: the differentiable '
                         'workload (200k keys, 1M queries in [0.1,0.9]^3, D=16, seed 3); '
@@ -403,7 +406,8 @@ def main():
 
     keys, queries, values = make_data(args, rank)
     t0 = time.perf_counter()
-    interp = ni.Interpolator(keys, device=dev, keep_host_mesh=(rank == 0 and not args.no_cpu_baseline))
+    interp = ni.Interpolator(keys, device=dev, keep_host_mesh=(rank == 0 and not args.no_cpu_baseline),
+                             predicates=args.predicates)
     build_s = time.perf_counter() - t0
     t0 = time.perf_counter()
     dm = interp.device_mesh
@@ -417,6 +421,7 @@ def main():
     # correctness gate on a sample before timing: bit-identical to the oracle
     sample_n = min(M, 20_000)
     om = oracle.OracleMesh(*interp.mesh_arrays)
+    om.set_predicates(args.predicates)
     Wref, stats, _ = om.weights(queries[:sample_n] - interp.centroid, with_stats=True)
     out_s = dm.interpolate(qd[:sample_n], vd, interp.centroid).cpu().numpy()
     exact = bool(np.array_equal(out_s, Wref @ values))
@@ -489,6 +494,7 @@ def main():
                       % (queries.nbytes / 1e6, dm.nbytes / 1e6),
                 'mesh_build_s': round(build_s, 2), 'mesh_upload_s': round(upload_s, 3),
                 'tets': dm.n_tets, 'bit_identical_to_oracle_on_sample': exact,
+                'predicates': args.predicates,
             },
             'roofline': {
                 'bound': 'fp64', 'kernel': 'k_rows_fast',

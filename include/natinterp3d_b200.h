@@ -109,9 +109,29 @@ int nif_dmesh_create(const double *d_vxyz, const int32_t *d_tet_v, const int32_t
 /* Frees the host handle (the device buffer belongs to the caller). */
 void nif_dmesh_destroy(nif_dmesh *m);
 
-/* Seed-grid dimensions and tet/vertex counts:
- * info = {n_vertices, n_tets, grid_x, grid_y, grid_z, 0, 0, 0}. */
+/* Seed-grid dimensions, tet/vertex counts and the predicate state:
+ * info = {n_vertices, n_tets, grid_x, grid_y, grid_z, orient_uncertain,
+ *         orient_flipped, predicate_mode}, where orient_uncertain counts the
+ * tets whose orient3dfast sign (natural_insertionfree.c:457-476) the static
+ * error bound cannot certify and orient_flipped those whose "> 0" flag the
+ * exact sign changes. */
 int nif_dmesh_info(const nif_dmesh *m, int64_t info[8]);
+
+/* Geometric predicates of later query calls on this mesh.  natinterp3d uses
+ * the signs of orient3dfast / inspherefast as they come (predicates.c:1687,
+ * 3301; natural_insertionfree.c:461-514, delaunay.c:400) and never calls its
+ * exact predicates; NIF_PRED_FAST (the default) does the same, bit for bit.
+ * NIF_PRED_AUDIT gives the same results and counts, in nif_summary, the
+ * evaluations whose fast value lies inside the static error bound
+ * (re-evaluated exactly) and those whose decision the exact sign would
+ * change.  NIF_PRED_EXACT decides every test by its exact sign (filter, then
+ * expansion arithmetic); a query exactly on a face or edge then floods its
+ * cavity from the lowest-id tet containing it.  A batch takes the modes its
+ * meshes have when nif_batch_create runs.  (No counterpart in natinterp3d.) */
+#define NIF_PRED_FAST 0
+#define NIF_PRED_AUDIT 1
+#define NIF_PRED_EXACT 2
+int nif_dmesh_set_predicates(nif_dmesh *m, int mode);
 
 /* Result summary of one query call (host memory). */
 typedef struct {
@@ -122,6 +142,14 @@ typedef struct {
     int64_t walk_steps;     /* total point-location steps */
     int32_t first_status;   /* status of a failing row, NIF_OK if none */
     int32_t reserved;
+    /* NIF_PRED_AUDIT / NIF_PRED_EXACT meshes, over the tests natinterp3d makes
+     * for these rows: walk orientation tests and cavity in-sphere tests whose
+     * fast value the error bound cannot certify, and those whose decision the
+     * exact sign changes.  The walk counts depend on the walk's seed tet. */
+    int64_t orient_uncertain;
+    int64_t orient_flipped;
+    int64_t insphere_uncertain;
+    int64_t insphere_flipped;
 } nif_summary;
 
 /* Device workspace bytes for M queries in the given mode
@@ -267,7 +295,7 @@ int nif_measure_fp64_peak(double *tflops_fused, double *tflops_separate);
  * host threads) race on it: serialise them.  Allocates no device or host
  * memory.  If summary is non-NULL the call synchronises `stream`. */
 #define NIF_NOALLOC_MAX_QUERIES (1 << 20)
-#define NIF_NOALLOC_SCRATCH_BYTES (16u << 20)
+#define NIF_NOALLOC_SCRATCH_BYTES (20u << 20)
 int nif_interpolate_noalloc(const nif_dmesh *m, const void *d_queries, int query_dtype, int64_t M,
                             const double centroid[3], const void *d_values, int values_dtype, int D,
                             void *d_out, int out_dtype, void *stream, nif_summary *summary);

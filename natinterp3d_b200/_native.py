@@ -152,13 +152,17 @@ NIF_F64 = 0
 NIF_F32 = 1
 NIF_MODE_WEIGHTS = 0
 NIF_MODE_INTERP = 1
+# predicate modes (nif_dmesh_set_predicates)
+PREDICATE_MODES = {'fast': 0, 'audit': 1, 'exact': 2}
 
 
 class Summary(ctypes.Structure):
     _fields_ = [('nnz', ctypes.c_int64), ('rows_large', ctypes.c_int64),
                 ('rows_failed', ctypes.c_int64), ('rows_outside', ctypes.c_int64),
                 ('walk_steps', ctypes.c_int64), ('first_status', ctypes.c_int32),
-                ('reserved', ctypes.c_int32)]
+                ('reserved', ctypes.c_int32), ('orient_uncertain', ctypes.c_int64),
+                ('orient_flipped', ctypes.c_int64), ('insphere_uncertain', ctypes.c_int64),
+                ('insphere_flipped', ctypes.c_int64)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_ if k != 'reserved'}
@@ -171,6 +175,7 @@ CUDA_SIGNATURES = {
                                  c_void_p, ctypes.POINTER(c_void_p)]),
     'nif_dmesh_destroy': (None, [c_void_p]),
     'nif_dmesh_info': (c_int, [c_void_p, ctypes.POINTER(c_int64)]),
+    'nif_dmesh_set_predicates': (c_int, [c_void_p, c_int]),
     'nif_query_workspace_bytes': (c_int, [c_void_p, c_int64, c_int, ctypes.POINTER(c_size_t)]),
     'nif_weights_count': (c_int, [c_void_p, c_void_p, c_int, c_int64, c_double_p, c_void_p,
                                   c_size_t, c_void_p, c_void_p, ctypes.POINTER(Summary)]),

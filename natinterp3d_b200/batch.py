@@ -25,14 +25,23 @@ __all__ = ['BatchInterpolator', 'BatchGraph']
 
 
 class BatchInterpolator:
-    def __init__(self, keys_list, device=None, threads=None):
+    """``predicates``: one mode for all problems ('fast', 'audit', 'exact'; see
+    :class:`Interpolator`) or a list with one mode per problem."""
+
+    def __init__(self, keys_list, device=None, threads=None, predicates='fast'):
         if not keys_list:
             raise ValueError('need at least one key set')
         threads = threads or min(len(keys_list), len(os.sched_getaffinity(0)))
         keys_list = [np.ascontiguousarray(k, np.float64) for k in keys_list]
+        modes = [predicates] * len(keys_list) if isinstance(predicates, str) else list(predicates)
+        if len(modes) != len(keys_list):
+            raise ValueError('need one predicate mode per problem')
         with ThreadPoolExecutor(max(1, threads)) as ex:
-            self.interpolators = list(ex.map(lambda k: Interpolator(k, device=device), keys_list))
+            self.interpolators = list(ex.map(
+                lambda km: Interpolator(km[0], device=device, predicates=km[1]),
+                zip(keys_list, modes)))
         self.P = len(self.interpolators)
+        # the batch records each mesh's predicate mode now (nif_batch_create)
         self.meshes = [it.device_mesh for it in self.interpolators]
         self.device = self.meshes[0].device
         self.n_keys = np.array([m.n_keys for m in self.meshes], np.int64)

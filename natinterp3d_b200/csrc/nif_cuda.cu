@@ -68,6 +68,9 @@ struct DevSummary {
     int first_status;
     int large_count;  // rows queued for the large kernel
     unsigned long long arena_used;
+    // predicate evaluations the filter could not certify / whose decision the
+    // exact sign changes (PRED_AUDIT and PRED_EXACT meshes)
+    unsigned long long orient_unc, orient_flip, insphere_unc, insphere_flip;
 };
 
 // ---------------------------------------------------------------------------
@@ -103,15 +106,22 @@ __global__ void k_prep_tets(const int32_t *__restrict__ tet_v, const int32_t *__
     }
 }
 
-// orientation flag, mirror slots, tet and face circumcentres
+// orientation flags, mirror slots, tet and face circumcentres.  flag[0]: bad
+// mesh, flag[1]: tets whose orientation sign the filter cannot certify.
 __global__ void k_prep_geometry(MeshView M, uint32_t *__restrict__ tinfo, d4 *__restrict__ tcc,
                                 d4 *__restrict__ fcc, int *__restrict__ bad) {
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < M.nt; t += gridDim.x * blockDim.x) {
         const int4 p = M.tv[t];
         const int4 n = M.tn[t];
         const dv3 P0 = vload(M, p.x), P1 = vload(M, p.y), P2 = vload(M, p.z), P3 = vload(M, p.w);
-        // natinterp3d recomputes this sign on every call (natural_insertionfree.c:457-476)
-        uint32_t info = orient_fast(P0, P1, P2, P3) > 0 ? 1u : 0u;
+        // natinterp3d recomputes this sign on every call (natural_insertionfree.c:457-476);
+        // bit 2 (the exact sign) equals it unless k_prep_exact_orient corrects it
+        const double o = orient_fast(P0, P1, P2, P3);
+        uint32_t info = o > 0 ? 5u : 0u;
+        if (orient_uncertain(P0, P1, P2, P3, o)) {
+            info |= 2u;
+            atomicAdd(&bad[1], 1);
+        }
         for (int j = 0; j < 4; j++) {
             const int nb = comp(n, j);
             int jm = 0;
@@ -140,6 +150,34 @@ __global__ void k_prep_geometry(MeshView M, uint32_t *__restrict__ tinfo, d4 *__
         fcc[4 * (size_t)t + 1] = d4{f1.x, f1.y, f1.z, 0.0};
         fcc[4 * (size_t)t + 2] = d4{f2.x, f2.y, f2.z, 0.0};
         fcc[4 * (size_t)t + 3] = d4{f3.x, f3.y, f3.z, 0.0};
+    }
+}
+
+// exact orientation (bit 2) of the tets flagged uncertain (bit 1); one warp
+// per block, lanes take turns in the block's scratch.  flag[2] counts the
+// tets whose "orient3d > 0" flag the exact sign changes.
+__global__ void __launch_bounds__(32) k_prep_exact_orient(MeshView M, uint32_t *__restrict__ tinfo,
+                                                          int *__restrict__ flag) {
+    __shared__ double scr[NIF_ORIENT_SCRATCH];
+    for (int base = blockIdx.x * 32; base < M.nt; base += gridDim.x * 32) {
+        const int t = base + threadIdx.x;
+        const bool unc = t < M.nt && (tinfo[t] & 2u);
+        unsigned um = __ballot_sync(0xffffffffu, unc);
+        while (um) {
+            const int l = __ffs(um) - 1;
+            um &= um - 1u;
+            if ((int)threadIdx.x == l) {
+                const int4 p = M.tv[t];
+                double a[3], b[3], c[3], d[3];
+                to3(vload(M, p.x), a), to3(vload(M, p.y), b), to3(vload(M, p.z), c);
+                to3(vload(M, p.w), d);
+                const uint32_t info = tinfo[t];
+                const uint32_t xpos = nif_orient_exact_sign(a, b, c, d, scr) > 0 ? 4u : 0u;
+                if ((xpos != 0) != ((info & 1u) != 0)) atomicAdd(&flag[2], 1);
+                tinfo[t] = (info & ~4u) | xpos;
+            }
+            __syncwarp();
+        }
     }
 }
 
@@ -721,8 +759,9 @@ __device__ __forceinline__ void record(DevSummary *sum, const RowInfo &r, int la
     if (r.outside) atomicAdd(&sum->rows_outside, 1ull);
 }
 
-// fast path: shared-memory scratch, rows in bucket order
-template <class QT, class Sink>
+// fast path: shared-memory scratch, rows in bucket order; PM is PM_PLAIN or
+// PM_FILTER
+template <class QT, class Sink, int PM>
 __global__ void __launch_bounds__(FAST_BLOCK, Sink::MIN_BLOCKS) k_rows_fast(MeshView M, const QT *__restrict__ Q,
                                                           Centroid cen, const int *__restrict__ order,
                                                           int64_t nrows, Sink sink, LargeQueue lq,
@@ -738,9 +777,9 @@ __global__ void __launch_bounds__(FAST_BLOCK, Sink::MIN_BLOCKS) k_rows_fast(Mesh
     for (int64_t s = gid; s < nrows; s += ng) {
         const int64_t i = order[s];
         const dv3 q = load_query(Q, i, cen.c);
-        const RowInfo r = sibson_row<G, typename std::remove_reference<decltype(ws)>::type, Sink::FULL>(M, q, ws, g);
+        const RowInfo r = sibson_row<G, FastWS, Sink::FULL, PM>(M, q, ws, g);
         steps += r.steps;
-        if (r.status == ST_CAPACITY) {
+        if (r.status == ST_CAPACITY || r.status == ST_UNCERTAIN) {
             if (g.lane == 0) {
                 const int slot = atomicAdd(&sum->large_count, 1);
                 lq.list[slot] = (int)i;
@@ -758,21 +797,33 @@ __global__ void __launch_bounds__(FAST_BLOCK, Sink::MIN_BLOCKS) k_rows_fast(Mesh
     if (g.lane == 0 && steps) atomicAdd(&sum->walk_steps, steps);
 }
 
-// large path: one warp per queued row, scratch in global memory
+template <int G>
+__device__ __forceinline__ void record_predicates(DevSummary *sum, const RowInfo &r, int lane) {
+    if (lane != 0) return;
+    if (r.o_unc) atomicAdd(&sum->orient_unc, (unsigned long long)r.o_unc);
+    if (r.o_flip) atomicAdd(&sum->orient_flip, (unsigned long long)r.o_flip);
+    if (r.i_unc) atomicAdd(&sum->insphere_unc, (unsigned long long)r.i_unc);
+    if (r.i_flip) atomicAdd(&sum->insphere_flip, (unsigned long long)r.i_flip);
+}
+
+// large path: one warp per queued row, scratch in global memory; resolves
+// uncertain predicates exactly (xs: NIF_EXACT_SCRATCH doubles per block)
 template <class QT, class Sink>
 __global__ void __launch_bounds__(32) k_rows_large(MeshView M, const QT *__restrict__ Q, Centroid cen,
                                                    LargeQueue lq, Sink sink, LargeWS *__restrict__ wsv,
-                                                   DevSummary *sum) {
+                                                   double *__restrict__ xsv, DevSummary *sum) {
     constexpr int G = LARGE_G;
     Grp<G> g;
     LargeWS &ws = wsv[blockIdx.x];
+    double *xs = xsv + (size_t)blockIdx.x * NIF_EXACT_SCRATCH;
     const int nq = sum->large_count;
     unsigned long long steps = 0;
     for (int j = blockIdx.x; j < nq; j += gridDim.x) {
         const int64_t i = lq.list[j];
         const dv3 q = load_query(Q, i, cen.c);
-        const RowInfo r = sibson_row<G, typename std::remove_reference<decltype(ws)>::type, Sink::FULL>(M, q, ws, g);
+        const RowInfo r = sibson_row<G, LargeWS, Sink::FULL, PM_RESOLVE>(M, q, ws, g, xs);
         steps += r.steps;
+        record_predicates<G>(sum, r, g.lane);
         if (g.lane == 0) atomicAdd(&sum->rows_large, 1ull);
         if (r.status != ST_OK) {
             if (g.lane == 0) {
@@ -847,6 +898,7 @@ struct nif_dmesh {
     int device;
     int num_sms;
     size_t bytes;
+    int64_t orient_unc, orient_flip;  // tets with an uncertain / flipped orientation flag
 };
 
 namespace {
@@ -923,6 +975,7 @@ struct QueryLayout {
     int64_t *scan_bsum;     // block sums for the scans
     int64_t *scan_total;
     LargeWS *large_ws;
+    double *exact;          // NIF_EXACT_SCRATCH doubles per large-row group
     // weights mode only
     int *cnt;
     int64_t *src, *off64;
@@ -951,6 +1004,7 @@ QueryLayout carve_query(Carve &c, int64_t M, int mode) {
     L.scan_bsum = c.take<int64_t>((mscan + SCAN_TILE - 1) / SCAN_TILE + 1);
     L.scan_total = c.take<int64_t>(1);
     L.large_ws = c.take<LargeWS>(LARGE_GROUPS);
+    L.exact = c.take<double>((size_t)LARGE_GROUPS * NIF_EXACT_SCRATCH);
     if (mode == NIF_MODE_WEIGHTS) {
         L.arena_cap = (int64_t)1 << 22;
         const int64_t stage = M * ROW_CAP + L.arena_cap;
@@ -1019,12 +1073,13 @@ void run_bucketing(const nif_dmesh *m, const QT *Q, int64_t M, const Centroid &c
     prof_mark(1, st);
 }
 
-template <class QT, class Sink>
-void run_rows(const nif_dmesh *m, const QT *Q, int64_t M, const Centroid &cen, const QueryLayout &L,
-              const Sink &sink, cudaStream_t st) {
+// persistent grid of the fast row kernel: resident blocks per SM x SMs
+template <class QT, class Sink, int PM>
+void launch_fast(const nif_dmesh *m, const QT *Q, int64_t M, const Centroid &cen,
+                 const QueryLayout &L, const Sink &sink, cudaStream_t st) {
     constexpr int GPB = FAST_BLOCK / FAST_G;
     const size_t smem = GPB * sizeof(FastWS);
-    auto kern = k_rows_fast<QT, Sink>;
+    auto kern = k_rows_fast<QT, Sink, PM>;
     static int per_sm = -1;  // resident blocks per SM of this instantiation
     if (per_sm < 0) {
         if (smem > 48 * 1024) set_smem(kern, smem);
@@ -1038,9 +1093,20 @@ void run_rows(const nif_dmesh *m, const QT *Q, int64_t M, const Centroid &cen, c
     if (blocks < 1) blocks = 1;
     kern<<<(unsigned)blocks, FAST_BLOCK, smem, st>>>(m->view, Q, cen, L.order, M, sink,
                                                     LargeQueue{L.large_list}, L.sum);
+}
+
+// fast rows (filtered when the mesh's predicate mode is not the default),
+// then the rows they queued; large_groups workspaces in L
+template <class QT, class Sink>
+void run_rows(const nif_dmesh *m, const QT *Q, int64_t M, const Centroid &cen, const QueryLayout &L,
+              const Sink &sink, cudaStream_t st, int large_groups = LARGE_GROUPS) {
+    if (m->view.pmode == PRED_FAST)
+        launch_fast<QT, Sink, PM_PLAIN>(m, Q, M, cen, L, sink, st);
+    else
+        launch_fast<QT, Sink, PM_FILTER>(m, Q, M, cen, L, sink, st);
     prof_mark(2, st);
-    k_rows_large<QT, Sink><<<LARGE_GROUPS, 32, 0, st>>>(m->view, Q, cen, LargeQueue{L.large_list},
-                                                        sink, L.large_ws, L.sum);
+    k_rows_large<QT, Sink><<<large_groups, 32, 0, st>>>(m->view, Q, cen, LargeQueue{L.large_list},
+                                                        sink, L.large_ws, L.exact, L.sum);
     prof_mark(3, st);
 }
 
@@ -1068,6 +1134,10 @@ int read_summary(const QueryLayout &L, cudaStream_t st, nif_summary *out, int64_
         out->walk_steps = (int64_t)d.walk_steps;
         out->first_status = d.first_status;
         out->reserved = 0;
+        out->orient_uncertain = (int64_t)d.orient_unc;
+        out->orient_flipped = (int64_t)d.orient_flip;
+        out->insphere_uncertain = (int64_t)d.insphere_unc;
+        out->insphere_flipped = (int64_t)d.insphere_flip;
     }
     if (total) *total = tot;
     return NIF_OK;
@@ -1130,6 +1200,7 @@ NIF_EXPORT int nif_dmesh_create(const double *d_vxyz, const int32_t *d_tet_v,
     V.n = n_vertices - 4;
     V.nv = n_vertices;
     V.nt = n_tets;
+    V.pmode = PRED_FAST;
 
     int rc = NIF_OK;
     do {
@@ -1149,6 +1220,17 @@ NIF_EXPORT int nif_dmesh_create(const double *d_vxyz, const int32_t *d_tet_v,
             break;
         }
         if (flag[0]) { rc = NIF_ERR_INTERNAL; break; }
+        h->orient_unc = flag[1];
+        if (flag[1] > 0) {
+            // rare: near-flat tets; resolve their exact orientation flags
+            k_prep_exact_orient<<<blocks_for(n_tets, 32, 4 * 148), 32, 0, st>>>(V, L.tinfo, L.flag);
+            if (cudaMemcpyAsync(flag, L.flag, sizeof(flag), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+                cudaStreamSynchronize(st) != cudaSuccess) {
+                rc = NIF_ERR_CUDA;
+                break;
+            }
+        }
+        h->orient_flip = flag[2];
         double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
         for (int b = 0; b < nbb; b++)
             for (int a = 0; a < 3; a++) {
@@ -1226,7 +1308,16 @@ NIF_EXPORT int nif_dmesh_info(const nif_dmesh *m, int64_t info[8]) {
     info[2] = m->view.gdim[0];
     info[3] = m->view.gdim[1];
     info[4] = m->view.gdim[2];
-    info[5] = info[6] = info[7] = 0;
+    info[5] = m->orient_unc;
+    info[6] = m->orient_flip;
+    info[7] = m->view.pmode;
+    return NIF_OK;
+}
+
+NIF_EXPORT int nif_dmesh_set_predicates(nif_dmesh *m, int mode) {
+    if (!m || (mode != NIF_PRED_FAST && mode != NIF_PRED_AUDIT && mode != NIF_PRED_EXACT))
+        return NIF_ERR_ARG;
+    m->view.pmode = mode;
     return NIF_OK;
 }
 
@@ -1447,30 +1538,8 @@ QueryLayout carve_noalloc(Carve &c, int64_t M) {
     L.scan_bsum = c.take<int64_t>((mscan + SCAN_TILE - 1) / SCAN_TILE + 1);
     L.scan_total = c.take<int64_t>(1);
     L.large_ws = c.take<LargeWS>(NOALLOC_LARGE_GROUPS);
+    L.exact = c.take<double>((size_t)NOALLOC_LARGE_GROUPS * NIF_EXACT_SCRATCH);
     return L;
-}
-
-template <class QT, class Sink>
-void noalloc_rows(const nif_dmesh *m, const QT *Q, int64_t M, const Centroid &cen,
-                  const QueryLayout &L, const Sink &sink, cudaStream_t st) {
-    constexpr int GPB = FAST_BLOCK / FAST_G;
-    const size_t smem = GPB * sizeof(FastWS);
-    auto kern = k_rows_fast<QT, Sink>;
-    static int per_sm = -1;
-    if (per_sm < 0) {
-        if (smem > 48 * 1024) set_smem(kern, smem);
-        per_sm = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, FAST_BLOCK, smem);
-        if (per_sm < 1) per_sm = 1;
-    }
-    int64_t blocks = (M + GPB - 1) / GPB;
-    const int64_t cap = (int64_t)per_sm * m->num_sms;
-    if (blocks > cap) blocks = cap;
-    if (blocks < 1) blocks = 1;
-    kern<<<(unsigned)blocks, FAST_BLOCK, smem, st>>>(m->view, Q, cen, L.order, M, sink,
-                                                    LargeQueue{L.large_list}, L.sum);
-    k_rows_large<QT, Sink><<<NOALLOC_LARGE_GROUPS, 32, 0, st>>>(
-        m->view, Q, cen, LargeQueue{L.large_list}, sink, L.large_ws, L.sum);
 }
 
 template <class QT, class VT, class CT>
@@ -1478,7 +1547,7 @@ void noalloc_typed(const nif_dmesh *m, const void *q, int64_t M, const Centroid 
                    const void *v, int D, void *out, const QueryLayout &L, cudaStream_t st) {
     InterpSink<QT, VT, CT> sink{static_cast<const VT *>(v), static_cast<CT *>(out), D};
     run_bucketing(m, static_cast<const QT *>(q), M, cen, L, st);
-    noalloc_rows(m, static_cast<const QT *>(q), M, cen, L, sink, st);
+    run_rows(m, static_cast<const QT *>(q), M, cen, L, sink, st, NOALLOC_LARGE_GROUPS);
 }
 
 }  // namespace
@@ -1787,7 +1856,7 @@ struct BatchInterpSink {
 // persistent row kernel of a batch: warps pull tiles of bucket-ordered
 // queries from a device counter; the mesh view of the current problem is
 // kept in shared memory
-template <class QT, class Sink>
+template <class QT, class Sink, int PM>
 __global__ void __launch_bounds__(FAST_BLOCK, Sink::MIN_BLOCKS)
     k_rows_batch(const MeshView *__restrict__ views, const int64_t *__restrict__ qoff, int P,
                  const QT *__restrict__ Q, const double *__restrict__ cens,
@@ -1820,9 +1889,9 @@ __global__ void __launch_bounds__(FAST_BLOCK, Sink::MIN_BLOCKS)
                 cur = p;
             }
             const dv3 q = load_query(Q, i, cens + 3 * p);
-            const RowInfo r = sibson_row<G, FastWS, Sink::FULL>(M, q, ws, g);
+            const RowInfo r = sibson_row<G, FastWS, Sink::FULL, PM>(M, q, ws, g);
             steps += r.steps;
-            if (r.status == ST_CAPACITY) {
+            if (r.status == ST_CAPACITY || r.status == ST_UNCERTAIN) {
                 if (g.lane == 0) {
                     const int slot = atomicAdd(&sum->large_count, 1);
                     lq.list[slot] = (int)i;
@@ -1847,11 +1916,12 @@ __global__ void __launch_bounds__(32) k_rows_batch_large(const MeshView *__restr
                                                          const QT *__restrict__ Q,
                                                          const double *__restrict__ cens, LargeQueue lq,
                                                          Sink sink, LargeWS *__restrict__ wsv,
-                                                         DevSummary *sum) {
+                                                         double *__restrict__ xsv, DevSummary *sum) {
     constexpr int G = LARGE_G;
     __shared__ MeshView M;
     Grp<G> g;
     LargeWS &ws = wsv[blockIdx.x];
+    double *xs = xsv + (size_t)blockIdx.x * NIF_EXACT_SCRATCH;
     const int nq = sum->large_count;
     int cur = -1;
     for (int j = blockIdx.x; j < nq; j += gridDim.x) {
@@ -1864,7 +1934,8 @@ __global__ void __launch_bounds__(32) k_rows_batch_large(const MeshView *__restr
             cur = p;
         }
         const dv3 q = load_query(Q, i, cens + 3 * p);
-        const RowInfo r = sibson_row<G, LargeWS, Sink::FULL>(M, q, ws, g);
+        const RowInfo r = sibson_row<G, LargeWS, Sink::FULL, PM_RESOLVE>(M, q, ws, g, xs);
+        record_predicates<G>(sum, r, g.lane);
         if (g.lane == 0) atomicAdd(&sum->rows_large, 1ull);
         if (r.status != ST_OK) {
             if (g.lane == 0) {
@@ -1885,6 +1956,7 @@ struct nif_dbatch {
     int P;
     int device;
     int num_sms;
+    bool filtered;      // some mesh uses a non-default predicate mode
     MeshView *d_views;  // [P] in the caller's buffer
 };
 
@@ -1896,6 +1968,7 @@ struct BatchLayout {
     int *bits, *bucket, *bcount, *order, *large_list, *bsum, *btotal;
     int64_t *bbase;
     LargeWS *large_ws;
+    double *exact;
 };
 
 BatchLayout carve_batch(Carve &c, int P, int64_t M) {
@@ -1912,7 +1985,29 @@ BatchLayout carve_batch(Carve &c, int P, int64_t M) {
     L.bsum = c.take<int>((nbk + 1 + SCAN_TILE - 1) / SCAN_TILE + 1);
     L.btotal = c.take<int>(2);
     L.large_ws = c.take<LargeWS>(LARGE_GROUPS);
+    L.exact = c.take<double>((size_t)LARGE_GROUPS * NIF_EXACT_SCRATCH);
     return L;
+}
+
+template <class QT, class Sink, int PM>
+void launch_batch_rows(const nif_dbatch *b, const QT *Q, int64_t M, const int64_t *qoff,
+                       const double *cens, const Sink &sink, const BatchLayout &L, cudaStream_t st) {
+    constexpr int GPB = FAST_BLOCK / FAST_G;
+    const size_t smem = GPB * sizeof(FastWS);
+    auto kern = k_rows_batch<QT, Sink, PM>;
+    static int per_sm = -1;
+    if (per_sm < 0) {
+        if (smem > 40 * 1024) set_smem(kern, smem);
+        per_sm = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, FAST_BLOCK, smem);
+        if (per_sm < 1) per_sm = 1;
+    }
+    const int64_t want = (M + (int64_t)GPB * BATCH_TILE - 1) / ((int64_t)GPB * BATCH_TILE);
+    int64_t blocks = (int64_t)per_sm * b->num_sms;
+    if (blocks > want) blocks = want;
+    if (blocks < 1) blocks = 1;
+    kern<<<(unsigned)blocks, FAST_BLOCK, smem, st>>>(b->d_views, qoff, b->P, Q, cens, L.order, M, sink,
+                                                    LargeQueue{L.large_list}, L.sum, L.counter);
 }
 
 template <class QT, class VT, class CT>
@@ -1931,25 +2026,13 @@ void batch_typed(const nif_dbatch *b, const void *q, int64_t M, const int64_t *q
     launch_scan<int>(L.bcount, nbk, L.bsum, L.btotal, L.bcount, st);
     k_scatter<<<blocks_for(M, 256), 256, 0, st>>>(L.bucket, M, L.bcount, L.order);
     Sink sink{static_cast<const VT *>(v), koff, qoff, b->P, static_cast<CT *>(out), D};
-    constexpr int GPB = FAST_BLOCK / FAST_G;
-    const size_t smem = GPB * sizeof(FastWS);
-    auto kern = k_rows_batch<QT, Sink>;
-    static int per_sm = -1;
-    if (per_sm < 0) {
-        if (smem > 40 * 1024) set_smem(kern, smem);
-        per_sm = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, FAST_BLOCK, smem);
-        if (per_sm < 1) per_sm = 1;
-    }
-    const int64_t want = (M + (int64_t)GPB * BATCH_TILE - 1) / ((int64_t)GPB * BATCH_TILE);
-    int64_t blocks = (int64_t)per_sm * b->num_sms;
-    if (blocks > want) blocks = want;
-    if (blocks < 1) blocks = 1;
-    kern<<<(unsigned)blocks, FAST_BLOCK, smem, st>>>(b->d_views, qoff, b->P, Q, cens, L.order, M, sink,
-                                                    LargeQueue{L.large_list}, L.sum, L.counter);
+    if (b->filtered)
+        launch_batch_rows<QT, Sink, PM_FILTER>(b, Q, M, qoff, cens, sink, L, st);
+    else
+        launch_batch_rows<QT, Sink, PM_PLAIN>(b, Q, M, qoff, cens, sink, L, st);
     k_rows_batch_large<QT, Sink><<<LARGE_GROUPS, 32, 0, st>>>(b->d_views, qoff, b->P, Q, cens,
                                                              LargeQueue{L.large_list}, sink,
-                                                             L.large_ws, L.sum);
+                                                             L.large_ws, L.exact, L.sum);
 }
 
 }  // namespace
@@ -1970,13 +2053,15 @@ NIF_EXPORT int nif_batch_create(int n_problems, nif_dmesh *const *meshes, void *
     MeshView *host = static_cast<MeshView *>(malloc(sizeof(MeshView) * (size_t)n_problems));
     if (!host) return NIF_ERR_NOMEM;
     int dev = -1;
+    bool filtered = false;
     for (int p = 0; p < n_problems; p++) {
         if (!meshes[p] || (p > 0 && meshes[p]->device != dev)) {
             free(host);
             return NIF_ERR_ARG;
         }
         dev = meshes[p]->device;
-        host[p] = meshes[p]->view;
+        host[p] = meshes[p]->view;  // predicate modes as of now
+        filtered = filtered || host[p].pmode != PRED_FAST;
     }
     cudaStream_t st = S(stream);
     if (cudaMemcpyAsync(d_buf, host, sizeof(MeshView) * (size_t)n_problems, cudaMemcpyHostToDevice, st) !=
@@ -1991,6 +2076,7 @@ NIF_EXPORT int nif_batch_create(int n_problems, nif_dmesh *const *meshes, void *
     b->P = n_problems;
     b->device = dev;
     b->num_sms = meshes[0]->num_sms;
+    b->filtered = filtered;
     b->d_views = static_cast<MeshView *>(d_buf);
     *out = b;
     return NIF_OK;
@@ -2061,6 +2147,10 @@ NIF_EXPORT int nif_batch_summary(const nif_dbatch *b, int64_t total_queries, con
     summary->walk_steps = (int64_t)d.walk_steps;
     summary->first_status = d.first_status;
     summary->reserved = 0;
+    summary->orient_uncertain = (int64_t)d.orient_unc;
+    summary->orient_flipped = (int64_t)d.orient_flip;
+    summary->insphere_uncertain = (int64_t)d.insphere_unc;
+    summary->insphere_flipped = (int64_t)d.insphere_flip;
     return NIF_OK;
 }
 

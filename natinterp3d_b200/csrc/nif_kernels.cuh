@@ -19,9 +19,23 @@
 // (computed with the same formulas and argument orders); a face shared by two
 // cavity tets uses the circumcentre computed from the tet natinterp3d visits
 // first, as natinterp3d's face cache does (:233-253).
+//
+// Predicates.  natinterp3d evaluates orient3dfast / inspherefast and uses their
+// signs as they come (predicates.c:1687, 3301); that is the default here
+// (PRED_FAST).  Two more modes per mesh: PRED_AUDIT keeps those signs and
+// counts every evaluation whose fast value the static error bound cannot
+// certify ("uncertain"), and those whose decision the exact sign would change
+// ("flipped"); PRED_EXACT decides by the exact sign.  The row routine comes in
+// three variants: PM_PLAIN (fast signs only), PM_FILTER (fast kernel of the
+// non-default modes: certified signs only, the row is handed to the
+// large-row kernel at the first uncertain evaluation that matters) and
+// PM_RESOLVE (large-row kernel: uncertain evaluations are resolved exactly,
+// one lane at a time, in a per-group global scratch, and counted).
 #pragma once
+#include <limits.h>
 #include <stdint.h>
 
+#include "nif_exact.h"
 #include "nif_geometry.cuh"
 
 namespace nif {
@@ -31,6 +45,17 @@ constexpr int ST_OK = 0;
 constexpr int ST_WALK = 1;       // walk step limit
 constexpr int ST_CAPACITY = 2;   // per-query capacity of this kernel exceeded
 constexpr int ST_ARENA = 3;      // large-row output arena full
+constexpr int ST_UNCERTAIN = 4;  // a predicate needs exact evaluation (PM_FILTER only)
+
+// predicate modes of a mesh (MeshView::pmode)
+constexpr int PRED_FAST = 0;
+constexpr int PRED_AUDIT = 1;
+constexpr int PRED_EXACT = 2;
+
+// row-routine variants
+constexpr int PM_PLAIN = 0;
+constexpr int PM_FILTER = 1;
+constexpr int PM_RESOLVE = 2;
 
 constexpr int WALK_LIMIT = 1 << 16;
 
@@ -43,12 +68,15 @@ struct MeshView {
     const d4 *__restrict__ vtx;        // [nv] x, y, z, 0
     const int4 *__restrict__ tv;       // [nt] vertex ids
     const int4 *__restrict__ tn;       // [nt] neighbour tets (-1 = none)
-    const uint32_t *__restrict__ tinfo;// [nt] bit0: orient3dfast(p0..p3) > 0; bits 8+2j: mirror slot of face j
+    const uint32_t *__restrict__ tinfo;// [nt] bit0: orient3dfast(p0..p3) > 0; bit1: that sign is
+                                       // uncertain; bit2: exact orient3d(p0..p3) > 0;
+                                       // bits 8+2j: mirror slot of face j
     const d4 *__restrict__ tcc;        // [nt] tet circumcentre
     const d4 *__restrict__ fcc;        // [nt*4] circumcentre of the face opposite p[i]
     const int *__restrict__ grid;      // seed tets of the finest grid level
     int n;                             // data vertices (ids >= n are super-simplex vertices)
     int nv, nt;
+    int pmode;                         // PRED_*
     int gdim[3];
     double glo[3], ginv[3];
 };
@@ -114,6 +142,9 @@ struct Grp {
     __device__ __forceinline__ int shfl(int v, int src) const { return __shfl_sync(mask, v, src, G); }
     __device__ __forceinline__ double shfl(double v, int src) const {
         return __shfl_sync(mask, v, src, G);
+    }
+    __device__ __forceinline__ int shfl_xor(int v, int off) const {
+        return __shfl_xor_sync(mask, v, off, G);
     }
 };
 
@@ -206,7 +237,114 @@ struct RowInfo {
     bool coincident;  // row from the coincident-vertex path
     double total;     // sum of the stolen volumes (the normaliser), 0 if none
     int nbf;          // boundary faces (ws.bface[0..nbf))
+    // PM_RESOLVE only: predicate evaluations natinterp3d performs for this row
+    // that the filter could not certify, and those whose decision the exact
+    // sign changes (walk orientation tests / cavity in-sphere tests)
+    int o_unc, o_flip, i_unc, i_flip;
 };
+
+// ---- predicate filters and exact resolution ---------------------------------
+__device__ __forceinline__ void to3(const dv3 &v, double *o) {
+    o[0] = v.x;
+    o[1] = v.y;
+    o[2] = v.z;
+}
+
+__device__ __forceinline__ int sgn(double x) { return (x > 0.0) - (x < 0.0); }
+
+__device__ __forceinline__ bool orient_uncertain(const dv3 &a, const dv3 &b, const dv3 &c,
+                                                 const dv3 &d, double fast) {
+    double pa[3], pb[3], pc[3], pd[3];
+    to3(a, pa), to3(b, pb), to3(c, pc), to3(d, pd);
+    return nif_orient_uncertain(fast, nif_orient_permanent(pa, pb, pc, pd));
+}
+
+__device__ __forceinline__ bool insphere_uncertain(const dv3 &a, const dv3 &b, const dv3 &c,
+                                                   const dv3 &d, const dv3 &e, double fast) {
+    double pa[3], pb[3], pc[3], pd[3], pe[3];
+    to3(a, pa), to3(b, pb), to3(c, pc), to3(d, pd), to3(e, pe);
+    return nif_insphere_uncertain(fast, nif_insphere_permanent(pa, pb, pc, pd, pe));
+}
+
+// Exact orient3d signs for the lanes with unc set, one lane at a time in the
+// shared scratch xs (NIF_EXACT_SCRATCH doubles); other lanes keep s.
+template <int G>
+__device__ __forceinline__ int resolve_orient(const Grp<G> &g, double *xs, bool unc, const dv3 &a,
+                                              const dv3 &b, const dv3 &c, const dv3 &d, int s) {
+    unsigned um = g.ballot(unc);
+    while (um) {
+        const int l = __ffs(um) - 1;
+        um &= um - 1u;
+        if (g.lane == l) {
+            double pa[3], pb[3], pc[3], pd[3];
+            to3(a, pa), to3(b, pb), to3(c, pc), to3(d, pd);
+            s = nif_orient_exact_sign(pa, pb, pc, pd, xs);
+        }
+        g.sync();
+    }
+    return s;
+}
+
+template <int G>
+__device__ __forceinline__ int resolve_insphere(const Grp<G> &g, double *xs, bool unc, const dv3 &a,
+                                                const dv3 &b, const dv3 &c, const dv3 &d,
+                                                const dv3 &e, int s) {
+    unsigned um = g.ballot(unc);
+    while (um) {
+        const int l = __ffs(um) - 1;
+        um &= um - 1u;
+        if (g.lane == l) {
+            double pa[3], pb[3], pc[3], pd[3], pe[3];
+            to3(a, pa), to3(b, pb), to3(c, pc), to3(d, pd), to3(e, pe);
+            s = nif_insphere_exact_sign(pa, pb, pc, pd, pe, xs);
+        }
+        g.sync();
+    }
+    return s;
+}
+
+// PRED_EXACT, query exactly on a face or edge of its located tet: the cavity
+// index of the lowest-id cavity tet whose closure contains q (exact signs),
+// from which the visiting order is replayed -- the order then no longer
+// depends on which of the containing tets the walk reached.
+template <int G, class W>
+__device__ int canonical_start(const MeshView &M, const W &ws, const Grp<G> &g, double *xs,
+                               const dv3 q, int ncav) {
+    int best_t = INT_MAX, best_c = 0;
+    for (int c0 = 0; c0 < ncav; c0 += G) {
+        const int c = c0 + g.lane;
+        bool alive = c < ncav;
+        const int tt = alive ? ws.cav_tet[c] : 0;
+        const int4 p = M.tv[tt];
+        for (int f = 0; f < 4; f++) {
+            dv3 v1{0.0, 0.0, 0.0}, v2 = v1, v3 = v1;
+            int s = 1;
+            bool unc = false;
+            if (alive) {
+                v1 = vload(M, comp(p, face_vslot(f, 0)));
+                v2 = vload(M, comp(p, face_vslot(f, 1)));
+                v3 = vload(M, comp(p, face_vslot(f, 2)));
+                const double o = orient_fast(v1, v2, v3, q);
+                s = sgn(o);
+                unc = orient_uncertain(v1, v2, v3, q, o);
+            }
+            s = resolve_orient(g, xs, unc, v1, v2, v3, q, s);
+            if (s < 0) alive = false;
+        }
+        if (alive && tt < best_t) {
+            best_t = tt;
+            best_c = c;
+        }
+    }
+    for (int off = G / 2; off > 0; off >>= 1) {
+        const int ot = g.shfl_xor(best_t, off), oc = g.shfl_xor(best_c, off);
+        if (ot < best_t) {
+            best_t = ot;
+            best_c = oc;
+        }
+    }
+    return best_c;
+}
 
 // Circumcentre natinterp3d's face cache returns for the face opposite p[i] of
 // cavity tet c (tet id t, tinfo word info): the value cached by whichever of
@@ -234,12 +372,18 @@ __device__ __forceinline__ int neighbour_slot(const W &ws, int v) {
 // with normalised weights ws.acc[0..nnb), in natinterp3d's column order.
 // With FULL = false only the combinatorial part is built (cavity, visiting
 // order, boundary faces, neighbours in column order) and no volume is
-// computed; the query-gradient kernel needs nothing more.
-template <int G, class W, bool FULL = true>
-__device__ RowInfo sibson_row(const MeshView &M, const dv3 q, W &ws, const Grp<G> &g) {
+// computed; the query-gradient kernel needs nothing more.  PM selects the
+// predicate variant (PM_*); PM_RESOLVE needs xs, NIF_EXACT_SCRATCH doubles of
+// global scratch owned by this group.
+template <int G, class W, bool FULL = true, int PM = PM_PLAIN>
+__device__ RowInfo sibson_row(const MeshView &M, const dv3 q, W &ws, const Grp<G> &g,
+                              double *xs = nullptr) {
     using cav_t = typename W::cav_t;
     using slot_t = typename W::slot_t;
-    RowInfo r{ST_OK, 0, 0, false, false, 0.0, 0};
+    RowInfo r{ST_OK, 0, 0, false, false, 0.0, 0, 0, 0, 0, 0};
+    // filters run only for the non-default modes
+    const bool filt = PM != PM_PLAIN && M.pmode != PRED_FAST;
+    bool on_face = false;  // PRED_EXACT: a face test of the located tet is exactly zero
 
     // ---- 1. point location -------------------------------------------------
     int t = M.grid[seed_cell(M, q)];
@@ -250,15 +394,43 @@ __device__ RowInfo sibson_row(const MeshView &M, const dv3 q, W &ws, const Grp<G
         }
         ++r.steps;
         const int4 p = M.tv[t];
-        bool neg = false;
+        int sg = 1;
+        bool unc = false;
+        dv3 v1{0.0, 0.0, 0.0}, v2 = v1, v3 = v1;
         if (g.lane < 4) {
             const int f = g.lane;
-            const dv3 v1 = vload(M, comp(p, face_vslot(f, 0)));
-            const dv3 v2 = vload(M, comp(p, face_vslot(f, 1)));
-            const dv3 v3 = vload(M, comp(p, face_vslot(f, 2)));
-            neg = orient_fast(v1, v2, v3, q) < 0;
+            v1 = vload(M, comp(p, face_vslot(f, 0)));
+            v2 = vload(M, comp(p, face_vslot(f, 1)));
+            v3 = vload(M, comp(p, face_vslot(f, 2)));
+            const double o = orient_fast(v1, v2, v3, q);
+            sg = sgn(o);
+            if (filt) unc = orient_uncertain(v1, v2, v3, q, o);
         }
-        const unsigned m = g.ballot(neg);
+        unsigned m;
+        if constexpr (PM == PM_PLAIN) {
+            m = g.ballot(sg < 0);
+        } else if constexpr (PM == PM_FILTER) {
+            // natinterp3d tests faces 0..3 and moves through the first negative
+            // one: only uncertain tests up to that face can change the step
+            m = g.ballot(!unc && sg < 0);
+            const int fn = m ? __ffs(m) - 1 : 4;
+            if (g.ballot(unc) & ((2u << fn) - 1u)) {
+                r.status = ST_UNCERTAIN;
+                return r;
+            }
+        } else {
+            if (filt) {
+                const int xsg = resolve_orient(g, xs, unc, v1, v2, v3, q, sg);
+                const int use = M.pmode == PRED_EXACT ? xsg : sg;
+                m = g.ballot(use < 0);
+                const unsigned seen = (2u << (m ? __ffs(m) - 1 : 3)) - 1u;  // tests natinterp3d makes
+                r.o_unc += __popc(g.ballot(unc) & seen);
+                r.o_flip += __popc(g.ballot(unc && ((xsg < 0) != (sg < 0))) & seen);
+                if (!m) on_face = g.ballot(use == 0) != 0u;
+            } else {
+                m = g.ballot(sg < 0);
+            }
+        }
         if (!m) break;
         const int nb = comp(M.tn[t], __ffs(m) - 1);
         if (nb < 0) {
@@ -286,16 +458,38 @@ __device__ RowInfo sibson_row(const MeshView &M, const dv3 q, W &ws, const Grp<G
     while (qhead < qtail) {
         const int n = min(G, qtail - qhead);
         int slot = -1, tt = -1;
-        bool inc = false;
+        bool inc = false, unc = false;
+        dv3 ia{0.0, 0.0, 0.0}, ib = ia, ic = ia, id = ia;
+        double sv = 0.0;
         if (g.lane < n) {
             slot = ws.u.a.queue[qhead + g.lane];
             tt = ws.u.a.hkey[slot];
             const int4 p = M.tv[tt];
-            const dv3 a = vload(M, p.x), b = vload(M, p.y), c = vload(M, p.z), d = vload(M, p.w);
+            const dv3 a = vload(M, p.x), b = vload(M, p.y);
+            ic = vload(M, p.z);
+            id = vload(M, p.w);
             // insphere argument order fixed by the tet's orientation
-            // (natural_insertionfree.c:511-515)
-            const bool pos = (M.tinfo[tt] & 1u) != 0;
-            inc = insphere_fast(pos ? a : b, pos ? b : a, c, d, q) > 0;
+            // (natural_insertionfree.c:511-515); PRED_EXACT uses the exact one
+            const uint32_t info = M.tinfo[tt];
+            const bool pos = (info & ((PM != PM_PLAIN && M.pmode == PRED_EXACT) ? 4u : 1u)) != 0;
+            ia = pos ? a : b;
+            ib = pos ? b : a;
+            sv = insphere_fast(ia, ib, ic, id, q);
+            inc = sv > 0;
+            if (filt) unc = insphere_uncertain(ia, ib, ic, id, q, sv);
+        }
+        if constexpr (PM == PM_FILTER) {
+            if (g.any(unc)) {
+                r.status = ST_UNCERTAIN;
+                return r;
+            }
+        } else if constexpr (PM == PM_RESOLVE) {
+            if (filt && g.any(unc)) {
+                const bool xin = resolve_insphere(g, xs, unc, ia, ib, ic, id, q, inc ? 1 : -1) > 0;
+                r.i_unc += __popc(g.ballot(unc));
+                r.i_flip += __popc(g.ballot(unc && xin != inc));
+                if (M.pmode == PRED_EXACT) inc = xin;
+            }
         }
         const unsigned cm = g.ballot(inc);
         const int ci = ncav + __popc(cm & g.lt());
@@ -373,12 +567,18 @@ __device__ RowInfo sibson_row(const MeshView &M, const dv3 q, W &ws, const Grp<G
     for (int c = g.lane; c < ncav; c += G) ws.pos[c] = (cav_t)-1;
     g.sync();
 
+    // cavity index 0 is the located tet, the flood's start
+    int start_c = 0;
+    if constexpr (PM == PM_RESOLVE) {
+        if (on_face && M.pmode == PRED_EXACT) start_c = canonical_start(M, ws, g, xs, q, ncav);
+    }
+
     // replay natinterp3d's LIFO flood on the cavity (its non-cavity tets are
     // leaves and do not change the order in which cavity tets are reached)
     if (g.lane == 0) {
         cav_t *stack = ws.u.r.stack;
         int sp = 0, nord = 0;
-        stack[sp++] = 0;
+        stack[sp++] = (cav_t)start_c;
         if constexpr (W::CAV <= 128) {
             // visited set in two 64-bit registers
             uint64_t v0 = 0, v1 = 0;

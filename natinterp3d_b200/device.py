@@ -65,6 +65,21 @@ class DeviceMesh:
         info = (ctypes.c_int64 * 8)()
         N.check(self._lib.nif_dmesh_info(self._h, info), 'nif_dmesh_info')
         self.grid_dims = (info[2], info[3], info[4])
+        # tets whose orient3dfast sign the error bound cannot certify, and
+        # those whose "> 0" flag the exact sign changes
+        self.orientation_stats = {'uncertain': int(info[5]), 'flipped': int(info[6])}
+        self.predicates = 'fast'
+        self.last_summary = None
+
+    def set_predicates(self, mode):
+        """'fast' (natinterp3d's signs, the default), 'audit' (the same
+        results, uncertain and flipped predicate evaluations counted in the
+        call summaries) or 'exact' (exact signs)."""
+        if mode not in N.PREDICATE_MODES:
+            raise ValueError("predicates must be one of 'fast', 'audit', 'exact'")
+        N.check(self._lib.nif_dmesh_set_predicates(self._h, N.PREDICATE_MODES[mode]),
+                'nif_dmesh_set_predicates')
+        self.predicates = mode
 
     @property
     def nbytes(self):
@@ -114,6 +129,7 @@ class DeviceMesh:
             if rc == N.NIF_ERR_OVERFLOW:
                 raise OverflowError('Total number of nonzero weights exceeds int32 limit')
             N.check(rc, 'nif_weights_count')
+            self.last_summary = summ.as_dict()
             self._raise_rows(summ)
             nnz = int(summ.nnz)
             # at least one element each, so the library always gets real pointers
@@ -161,6 +177,8 @@ class DeviceMesh:
                                               ws.numel(), _stream_ptr(self.device),
                                               ctypes.byref(summ) if want else None),
                     'nif_interpolate')
+            if want:
+                self.last_summary = summ.as_dict()
             if check:
                 self._raise_rows(summ)
         out = out[:, 0] if squeeze else out
@@ -172,13 +190,19 @@ class DeviceMesh:
 
     def raise_pending(self, pending):
         """Read the row counters of interpolate(..., sync=False) calls (after they
-        ran) and raise if any row failed."""
+        ran), keep their sum as ``last_summary`` and raise if any row failed."""
+        total = None
         for M, ws in pending:
             summ = N.Summary()
             N.check(self._lib.nif_query_summary(self._h, int(M), N.NIF_MODE_INTERP, _vp(ws),
                                                 ws.numel(), _stream_ptr(self.device),
                                                 ctypes.byref(summ)), 'nif_query_summary')
+            d = summ.as_dict()
+            total = d if total is None else {k: (v + d[k] if k != 'first_status' else v or d[k])
+                                             for k, v in total.items()}
             self._raise_rows(summ)
+        if total is not None:
+            self.last_summary = total
 
     # -------------------------------------------------------------- sparse / grad
     def spmm(self, rowptr, cols, vals, x):

@@ -15,6 +15,11 @@ Same names, arguments, return types and errors:
 effect.  ``device`` selects the CUDA device (default: the current one).
 There is no CPU fallback: without a CUDA device the query methods raise.
 
+``predicates`` (an extension) selects the geometric predicates: 'fast' is
+natinterp3d's behaviour and the default; 'audit' gives identical results and
+counts the predicate evaluations that the static error bound cannot certify
+(``predicate_stats``); 'exact' decides them exactly.
+
 Device-resident variants (``get_weights_device``, ``interpolate_device``)
 take and return torch tensors on the mesh's GPU.
 """
@@ -72,6 +77,7 @@ class Interpolator:
         device: CUDA device for the resident mesh (default: current device).
         keep_host_mesh: keep natinterp3d's host mesh object alive (only needed
             to run natinterp3d's CPU query on the same mesh for comparison).
+        predicates: 'fast' (natinterp3d's non-robust signs), 'audit' or 'exact'.
     """
 
     def __init__(
@@ -81,6 +87,7 @@ class Interpolator:
         num_threads: Optional[int] = None,
         device=None,
         keep_host_mesh: bool = False,
+        predicates: str = 'fast',
     ):
         data_points = np.ascontiguousarray(data_points, np.float64)
         if data_points.ndim != 2 or data_points.shape[1] != 3:
@@ -99,9 +106,11 @@ class Interpolator:
             host.close()
         self._device_arg = device
         self._dmesh = None
+        self._predicates = 'fast'
+        self.set_predicates(predicates)
 
     @classmethod
-    def from_mesh(cls, centroid, vxyz, tet_v, tet_n, device=None):
+    def from_mesh(cls, centroid, vxyz, tet_v, tet_n, device=None, predicates='fast'):
         """An interpolator over an already exported mesh (see :meth:`save_mesh`)."""
         self = cls.__new__(cls)
         self._centroid = np.asarray(centroid, np.float64).reshape(3)
@@ -114,6 +123,8 @@ class Interpolator:
         self.host_mesh = None
         self._device_arg = device
         self._dmesh = None
+        self._predicates = 'fast'
+        self.set_predicates(predicates)
         return self
 
     def save_mesh(self, path):
@@ -134,7 +145,35 @@ class Interpolator:
     def device_mesh(self) -> DeviceMesh:
         if self._dmesh is None:
             self._dmesh = DeviceMesh(*self.mesh_arrays, device=self._device_arg)
+            self._dmesh.set_predicates(self._predicates)
         return self._dmesh
+
+    def set_predicates(self, mode):
+        """'fast', 'audit' or 'exact' for the following calls."""
+        if mode not in ('fast', 'audit', 'exact'):
+            raise ValueError("predicates must be one of 'fast', 'audit', 'exact'")
+        self._predicates = mode
+        if self._dmesh is not None:
+            self._dmesh.set_predicates(mode)
+
+    @property
+    def predicates(self):
+        return self._predicates
+
+    @property
+    def predicate_stats(self):
+        """Counters of the last query call ('audit' and 'exact' modes): walk
+        orientation and cavity in-sphere tests natinterp3d makes whose fast
+        value the error bound cannot certify (*_uncertain) and those whose
+        decision the exact sign changes (*_flipped); plus the mesh's tets with
+        an uncertain / flipped orientation flag."""
+        dm = self.device_mesh
+        s = dm.last_summary or {}
+        keys = ('orient_uncertain', 'orient_flipped', 'insphere_uncertain', 'insphere_flipped')
+        out = {k: int(s.get(k, 0)) for k in keys}
+        out['tets_orientation_uncertain'] = dm.orientation_stats['uncertain']
+        out['tets_orientation_flipped'] = dm.orientation_stats['flipped']
+        return out
 
     @property
     def device(self):

@@ -51,12 +51,17 @@ def _stale(target, sources):
     return any(os.path.getmtime(s) > t for s in sources if os.path.exists(s))
 
 
+# the exact-predicate arithmetic shared with the product (nif_exact.h)
+EXACT_DIR = os.path.join(os.path.dirname(HERE), 'natinterp3d_b200', 'csrc')
+
+
 def build_oracle(force=False):
     os.makedirs(LIB_DIR, exist_ok=True)
     src = os.path.join(HERE, 'nif_oracle.c')
-    if force or _stale(ORACLE_SO, [src, __file__]):
+    deps = [src, __file__, os.path.join(EXACT_DIR, 'nif_exact.h')]
+    if force or _stale(ORACLE_SO, deps):
         _run([_cc(), '-O2', '-std=c11', '-ffp-contract=off', '-fno-fast-math', '-fPIC',
-              '-shared', '-Wall', '-o', ORACLE_SO, src, '-lm'])
+              '-shared', '-Wall', '-I', EXACT_DIR, '-o', ORACLE_SO, src, '-lm'])
     return ORACLE_SO
 
 

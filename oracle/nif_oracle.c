@@ -17,6 +17,19 @@
  * finds the same exact-nearest centroid with a uniform grid (ties go to the
  * lowest tet id).  The walk, cavity search, boundary extraction, neighbour
  * order, volume terms and normalisation follow natinterp3d step by step.
+ *
+ * Predicate modes (orc_mesh_set_predicates), the same three the product has:
+ *   0  natinterp3d's signs: the fast determinants' own signs (the default);
+ *   1  the same signs, and every evaluation whose fast value lies inside the
+ *      static error bound is re-evaluated exactly and counted ("uncertain"),
+ *      together with those whose decision the exact sign would change
+ *      ("flipped");
+ *   2  exact signs (filter, then expansion arithmetic), counted the same
+ *      way; a query that lies exactly on a face or edge of the tet its walk
+ *      ends in floods the cavity from the lowest-id tet containing it, so
+ *      the visiting order does not depend on the walk's seed.
+ * The exact arithmetic is the product's nif_exact.h, pinned separately
+ * against rational arithmetic and against Shewchuk's robust predicates.
  */
 #include <math.h>
 #include <stdint.h>
@@ -28,6 +41,12 @@
 #define ORC_ERR_NOMEM -3
 #define ORC_ERR_OVERFLOW -5
 #define ORC_ERR_WALK -6
+
+#define ORC_PRED_FAST 0
+#define ORC_PRED_AUDIT 1
+#define ORC_PRED_EXACT 2
+
+#include "nif_exact.h"
 
 /* ------------------------------------------------------------------------- */
 /* Geometric predicates: the non-robust "fast" determinants natinterp3d calls  */
@@ -149,6 +168,11 @@ typedef struct {
     const int32_t *tv;       /* [nt][4] */
     const int32_t *tn;       /* [nt][4] */
     unsigned char *pos;      /* orient3dfast(p0..p3) > 0, natural_insertionfree.c:457-476 */
+    unsigned char *pos_x;    /* exact orient3d(p0..p3) > 0 */
+    long orient_unc, orient_flip; /* tets whose orientation sign is uncertain / flipped */
+    int pmode;               /* ORC_PRED_* */
+    int seed_first;          /* walk from tet 0, as natinterp3d does without its k-d tree
+                                (delaunay.c:389-391), instead of the nearest centroid */
     double *cen;             /* tet centroids [nt][3], delaunay.c:152-157 */
     /* exact nearest-centroid grid */
     double lo[3], h[3];
@@ -173,6 +197,7 @@ static int cell_coord(const orc_mesh *m, int d, double x) {
 void orc_mesh_free(orc_mesh *m) {
     if (!m) return;
     free(m->pos);
+    free(m->pos_x);
     free(m->cen);
     free(m->cell_start);
     free(m->cell_items);
@@ -186,12 +211,22 @@ orc_mesh *orc_mesh_new(const double *vx, int nv, const int32_t *tv, const int32_
     m->nv = nv; m->nt = nt; m->n = nv - 4;
     m->vx = vx; m->tv = tv; m->tn = tn;
     m->pos = malloc((size_t)nt);
+    m->pos_x = malloc((size_t)nt);
     m->cen = malloc(sizeof(double) * 3 * (size_t)nt);
-    if (!m->pos || !m->cen) { orc_mesh_free(m); return NULL; }
+    if (!m->pos || !m->pos_x || !m->cen) { orc_mesh_free(m); return NULL; }
+    double oscr[NIF_ORIENT_SCRATCH];
     double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
     for (int t = 0; t < nt; t++) {
         const int32_t *p = tv + 4 * (size_t)t;
-        m->pos[t] = orc_orient(V(m, p[0]), V(m, p[1]), V(m, p[2]), V(m, p[3])) > 0;
+        const double *P0 = V(m, p[0]), *P1 = V(m, p[1]), *P2 = V(m, p[2]), *P3 = V(m, p[3]);
+        const double o = orc_orient(P0, P1, P2, P3);
+        m->pos[t] = o > 0;
+        m->pos_x[t] = m->pos[t];
+        if (nif_orient_uncertain(o, nif_orient_permanent(P0, P1, P2, P3))) {
+            m->orient_unc++;
+            m->pos_x[t] = nif_orient_exact_sign(P0, P1, P2, P3, oscr) > 0;
+            if (m->pos_x[t] != m->pos[t]) m->orient_flip++;
+        }
         for (int d = 0; d < 3; d++) {
             double c = (V(m, p[0])[d] + V(m, p[1])[d] + V(m, p[2])[d] + V(m, p[3])[d]) / 4;
             m->cen[3 * (size_t)t + d] = c;
@@ -289,27 +324,6 @@ static int nearest_centroid(const orc_mesh *m, const double *q) {
     return best;
 }
 
-/* findContainingSimplex, delaunay.c:383-407 (walk with the first face whose
- * orient3dfast is negative, restarting from face 0 after every step).
- * Returns the tet, -1 outside the super-simplex, -2 on step-limit. */
-static int locate(const orc_mesh *m, const double *q, long *steps) {
-    int t = nearest_centroid(m, q);
-    long cap = 4L * m->nt + 1024;
-    for (long it = 0; it < cap; it++) {
-        const int32_t *p = m->tv + 4 * (size_t)t;
-        int f = 0;
-        for (; f < 4; f++) {
-            if (orc_orient(V(m, p[FACE3[f][0]]), V(m, p[FACE3[f][1]]), V(m, p[FACE3[f][2]]), q) < 0)
-                break;
-        }
-        if (f == 4) { if (steps) *steps += it + 1; return t; }
-        int nb = m->tn[4 * (size_t)t + f];
-        if (nb < 0) { if (steps) *steps += it + 1; return -1; }
-        t = nb;
-    }
-    return -2;
-}
-
 /* ------------------------------------------------------------------------- */
 /* Per-query scratch                                                          */
 /* ------------------------------------------------------------------------- */
@@ -338,12 +352,13 @@ typedef struct {
     int stolen_cap;
     fcc_entry *fcc;
     int fcc_size;
+    double *xs;           /* exact-predicate scratch, NIF_EXACT_SCRATCH doubles */
 } orc_scratch;
 
 static void scratch_free(orc_scratch *s) {
     free(s->tet_seen); free(s->tet_cav); free(s->slot_of);
     free(s->stack.a); free(s->cavity.a); free(s->bface_t.a); free(s->bface_f.a); free(s->nbr.a);
-    free(s->stolen); free(s->fcc);
+    free(s->stolen); free(s->fcc); free(s->xs);
 }
 
 static int scratch_init(orc_scratch *s, const orc_mesh *m) {
@@ -351,7 +366,8 @@ static int scratch_init(orc_scratch *s, const orc_mesh *m) {
     s->tet_seen = calloc((size_t)m->nt, sizeof(unsigned));
     s->tet_cav = calloc((size_t)m->nt, sizeof(unsigned));
     s->slot_of = malloc(sizeof(int) * (size_t)m->nv);
-    if (!s->tet_seen || !s->tet_cav || !s->slot_of) return -1;
+    s->xs = malloc(sizeof(double) * NIF_EXACT_SCRATCH);
+    if (!s->tet_seen || !s->tet_cav || !s->slot_of || !s->xs) return -1;
     for (int i = 0; i < m->nv; i++) s->slot_of[i] = -1;
     s->gen = 0;
     return 0;
@@ -384,7 +400,80 @@ static const v3 *fcc_lookup(orc_scratch *s, const orc_mesh *m, int a, int b, int
 typedef struct {
     long queries, walk_steps, insphere, cavity, boundary, neighbours;
     long old_terms, new_terms, face_cc, coincident, outside, empty, errors;
+    long orient_unc, orient_flip, insphere_unc, insphere_flip;
 } orc_stats;
+
+/* Sign of orient3d(a, b, c, q) under the mesh's predicate mode.  Counts the
+ * evaluation in st (when non-NULL) if the filter cannot certify it. */
+static int pred_orient(const orc_mesh *m, orc_scratch *s, orc_stats *st, const double *a,
+                       const double *b, const double *c, const double *q) {
+    const double o = orc_orient(a, b, c, q);
+    const int fs = o > 0 ? 1 : (o < 0 ? -1 : 0);
+    if (m->pmode == ORC_PRED_FAST || !nif_orient_uncertain(o, nif_orient_permanent(a, b, c, q)))
+        return fs;
+    const int xs = nif_orient_exact_sign(a, b, c, q, s->xs);
+    if (st) {
+        st->orient_unc++;
+        if ((xs < 0) != (fs < 0)) st->orient_flip++;
+    }
+    return m->pmode == ORC_PRED_EXACT ? xs : fs;
+}
+
+/* "inside the circumsphere" decision for tet t (inspherefast(...) > 0 with
+ * the argument order fixed by the tet's orientation,
+ * natural_insertionfree.c:511-515) under the mesh's predicate mode */
+static int pred_in_cavity(const orc_mesh *m, orc_scratch *s, orc_stats *st, int t,
+                          const double *q) {
+    const int32_t *p = m->tv + 4 * (size_t)t;
+    const int pos = m->pmode == ORC_PRED_EXACT ? m->pos_x[t] : m->pos[t];
+    const double *a = V(m, pos ? p[0] : p[1]), *b = V(m, pos ? p[1] : p[0]);
+    const double *c = V(m, p[2]), *d = V(m, p[3]);
+    const double v = orc_insphere(a, b, c, d, q);
+    if (m->pmode == ORC_PRED_FAST || !nif_insphere_uncertain(v, nif_insphere_permanent(a, b, c, d, q)))
+        return v > 0;
+    const int xs = nif_insphere_exact_sign(a, b, c, d, q, s->xs);
+    if (st) {
+        st->insphere_unc++;
+        if ((xs > 0) != (v > 0)) st->insphere_flip++;
+    }
+    return m->pmode == ORC_PRED_EXACT ? xs > 0 : v > 0;
+}
+
+/* findContainingSimplex, delaunay.c:383-407 (walk with the first face whose
+ * orient3d is negative, restarting from face 0 after every step).  Returns
+ * the tet, -1 outside the super-simplex, -2 on step-limit; *on_face is set
+ * when a face test of the final tet came out exactly zero. */
+static int locate(const orc_mesh *m, const double *q, long *steps, orc_scratch *s,
+                  orc_stats *st, int *on_face) {
+    int t = m->seed_first ? 0 : nearest_centroid(m, q);
+    long cap = 4L * m->nt + 1024;
+    *on_face = 0;
+    for (long it = 0; it < cap; it++) {
+        const int32_t *p = m->tv + 4 * (size_t)t;
+        int f = 0, zero = 0;
+        for (; f < 4; f++) {
+            const int sg = pred_orient(m, s, st, V(m, p[FACE3[f][0]]), V(m, p[FACE3[f][1]]),
+                                       V(m, p[FACE3[f][2]]), q);
+            if (sg < 0) break;
+            if (sg == 0) zero = 1;
+        }
+        if (f == 4) { if (steps) *steps += it + 1; *on_face = zero; return t; }
+        int nb = m->tn[4 * (size_t)t + f];
+        if (nb < 0) { if (steps) *steps += it + 1; return -1; }
+        t = nb;
+    }
+    return -2;
+}
+
+/* 1 if q lies in the closed tet t (every face test >= 0), exact-mode signs */
+static int tet_contains(const orc_mesh *m, orc_scratch *s, int t, const double *q) {
+    const int32_t *p = m->tv + 4 * (size_t)t;
+    for (int f = 0; f < 4; f++)
+        if (pred_orient(m, s, NULL, V(m, p[FACE3[f][0]]), V(m, p[FACE3[f][1]]),
+                        V(m, p[FACE3[f][2]]), q) < 0)
+            return 0;
+    return 1;
+}
 
 static int slot_add(orc_scratch *s, int vid) {
     if (s->slot_of[vid] >= 0) return s->slot_of[vid];
@@ -404,42 +493,25 @@ static int slot_add(orc_scratch *s, int vid) {
 
 /* getWeightsSingleQueryIF, natural_insertionfree.c:591-738.  Leaves the row
  * in s->nbr / s->stolen (neighbour count s->nbr.n).  Returns 0 or an error. */
-static int query_one(const orc_mesh *m, const double *q, orc_scratch *s, orc_stats *st) {
-    for (int i = 0; i < s->nbr.n; i++) s->slot_of[s->nbr.a[i]] = -1;
-    s->nbr.n = 0;
-    s->cavity.n = 0;
-    s->bface_t.n = 0;
-    s->bface_f.n = 0;
+/* findCavity (natural_insertionfree.c:486-551): LIFO flood from start; a tet
+ * joins the cavity iff it passes the in-sphere decision; neighbours are
+ * pushed in slot order 0..3.  Evaluations are counted in st when non-NULL. */
+static int flood(const orc_mesh *m, const double *q, orc_scratch *s, orc_stats *st, int start) {
     if (++s->gen == 0) {
         memset(s->tet_seen, 0, sizeof(unsigned) * (size_t)m->nt);
         memset(s->tet_cav, 0, sizeof(unsigned) * (size_t)m->nt);
         s->gen = 1;
     }
     const unsigned g = s->gen;
-
-    long steps = 0;
-    int start = locate(m, q, &steps);
-    st->walk_steps += steps;
-    if (start == -2) { st->errors++; return ORC_ERR_WALK; }
-    if (start == -1) { st->outside++; return ORC_OK; }
-
-    /* findCavity (natural_insertionfree.c:486-551): LIFO flood; a tet joins
-     * the cavity iff inspherefast(...) > 0 with the argument order fixed by
-     * its orientation sign; neighbours are pushed in slot order 0..3. */
+    s->cavity.n = 0;
     s->stack.n = 0;
     if (ipush(&s->stack, start)) return ORC_ERR_NOMEM;
     while (s->stack.n > 0) {
         int t = s->stack.a[--s->stack.n];
         if (s->tet_seen[t] == g) continue;
         s->tet_seen[t] = g;
-        const int32_t *p = m->tv + 4 * (size_t)t;
-        double ins;
-        if (m->pos[t])
-            ins = orc_insphere(V(m, p[0]), V(m, p[1]), V(m, p[2]), V(m, p[3]), q);
-        else
-            ins = orc_insphere(V(m, p[1]), V(m, p[0]), V(m, p[2]), V(m, p[3]), q);
-        st->insphere++;
-        if (ins > 0) {
+        if (st) st->insphere++;
+        if (pred_in_cavity(m, s, st, t, q)) {
             if (ipush(&s->cavity, t)) return ORC_ERR_NOMEM;
             s->tet_cav[t] = g;
             for (int i = 0; i < 4; i++) {
@@ -449,6 +521,41 @@ static int query_one(const orc_mesh *m, const double *q, orc_scratch *s, orc_sta
             }
         }
     }
+    return ORC_OK;
+}
+
+/* getWeightsSingleQueryIF, natural_insertionfree.c:591-738.  Leaves the row
+ * in s->nbr / s->stolen (neighbour count s->nbr.n).  Returns 0 or an error. */
+static int query_one(const orc_mesh *m, const double *q, orc_scratch *s, orc_stats *st) {
+    for (int i = 0; i < s->nbr.n; i++) s->slot_of[s->nbr.a[i]] = -1;
+    s->nbr.n = 0;
+    s->cavity.n = 0;
+    s->bface_t.n = 0;
+    s->bface_f.n = 0;
+
+    long steps = 0;
+    int on_face = 0;
+    int start = locate(m, q, &steps, s, st, &on_face);
+    st->walk_steps += steps;
+    if (start == -2) { st->errors++; return ORC_ERR_WALK; }
+    if (start == -1) { st->outside++; return ORC_OK; }
+
+    int rc = flood(m, q, s, st, start);
+    if (rc) return rc;
+    if (m->pmode == ORC_PRED_EXACT && on_face && s->cavity.n > 0) {
+        /* canonical start: the lowest-id cavity tet that contains q */
+        int best = -1;
+        for (int ci = 0; ci < s->cavity.n; ci++) {
+            const int t = s->cavity.a[ci];
+            if ((best < 0 || t < best) && tet_contains(m, s, t, q)) best = t;
+        }
+        if (best >= 0 && best != start) {
+            start = best;
+            rc = flood(m, q, s, NULL, start);
+            if (rc) return rc;
+        }
+    }
+    const unsigned g = s->gen;
     st->cavity += s->cavity.n;
 
     if (s->cavity.n == 0) {
@@ -573,7 +680,7 @@ void orc_free(void *p) { free(p); }
 /* queries: [M][3] centred float64.  rowptr: caller-provided int32[M+1].
  * *vals / *cols are malloc'd here (free with orc_free).  status (optional,
  * int8[M]) receives 0 or the per-row error.  stats (optional) gets counters
- * as 13 int64 values in orc_stats order. */
+ * as 17 int64 values in orc_stats order. */
 int orc_weights(const orc_mesh *m, const double *queries, int M, double **vals, int **cols,
                 int *rowptr, signed char *status, long *stats) {
     if (!m || (!queries && M > 0) || M < 0 || !vals || !cols || !rowptr) return ORC_ERR_ARG;
@@ -619,7 +726,8 @@ int orc_weights(const orc_mesh *m, const double *queries, int M, double **vals, 
         o[0] = st.queries; o[1] = st.walk_steps; o[2] = st.insphere; o[3] = st.cavity;
         o[4] = st.boundary; o[5] = st.neighbours; o[6] = st.old_terms; o[7] = st.new_terms;
         o[8] = st.face_cc; o[9] = st.coincident; o[10] = st.outside; o[11] = st.empty;
-        o[12] = st.errors;
+        o[12] = st.errors; o[13] = st.orient_unc; o[14] = st.orient_flip;
+        o[15] = st.insphere_unc; o[16] = st.insphere_flip;
     }
     return ORC_OK;
 }
@@ -659,4 +767,51 @@ void orc_tet_geometry(const orc_mesh *m, unsigned char *pos, double *tcc, double
             }
         }
     }
+}
+
+/* predicate mode of later orc_weights calls: ORC_PRED_FAST/AUDIT/EXACT */
+int orc_mesh_set_predicates(orc_mesh *m, int mode) {
+    if (!m || mode < ORC_PRED_FAST || mode > ORC_PRED_EXACT) return ORC_ERR_ARG;
+    m->pmode = mode;
+    return ORC_OK;
+}
+
+/* walk seed of later orc_weights calls: 0 nearest tet centroid (natinterp3d's
+ * k-d tree seed, the default), 1 tet 0 (natinterp3d without a k-d tree) */
+int orc_mesh_set_seed(orc_mesh *m, int first_tet) {
+    if (!m) return ORC_ERR_ARG;
+    m->seed_first = first_tet != 0;
+    return ORC_OK;
+}
+
+/* tets whose orientation sign the filter could not certify, and those whose
+ * "orient3d > 0" flag the exact sign changes */
+void orc_mesh_predicate_info(const orc_mesh *m, long out[2]) {
+    out[0] = m->orient_unc;
+    out[1] = m->orient_flip;
+}
+
+/* the exact arithmetic and filters on their own, for known-answer tests */
+int orc_orient_exact_sign(const double *a, const double *b, const double *c, const double *d) {
+    double s[NIF_ORIENT_SCRATCH];
+    return nif_orient_exact_sign(a, b, c, d, s);
+}
+
+int orc_insphere_exact_sign(const double *a, const double *b, const double *c, const double *d,
+                            const double *e) {
+    double *s = malloc(sizeof(double) * NIF_EXACT_SCRATCH);
+    if (!s) return -2;
+    int r = nif_insphere_exact_sign(a, b, c, d, e, s);
+    free(s);
+    return r;
+}
+
+int orc_orient_uncertain(const double *a, const double *b, const double *c, const double *d) {
+    return nif_orient_uncertain(orc_orient(a, b, c, d), nif_orient_permanent(a, b, c, d));
+}
+
+int orc_insphere_uncertain(const double *a, const double *b, const double *c, const double *d,
+                           const double *e) {
+    return nif_insphere_uncertain(orc_insphere(a, b, c, d, e),
+                                  nif_insphere_permanent(a, b, c, d, e));
 }

@@ -21,7 +21,10 @@ c_int_p = ctypes.POINTER(ctypes.c_int)
 c_void_p = ctypes.c_void_p
 
 STATS_FIELDS = ('queries', 'walk_steps', 'insphere', 'cavity', 'boundary', 'neighbours',
-                'old_terms', 'new_terms', 'face_cc', 'coincident', 'outside', 'empty', 'errors')
+                'old_terms', 'new_terms', 'face_cc', 'coincident', 'outside', 'empty', 'errors',
+                'orient_uncertain', 'orient_flipped', 'insphere_uncertain', 'insphere_flipped')
+
+PREDICATE_MODES = {'fast': 0, 'audit': 1, 'exact': 2}
 
 _olib = None
 _rlib = None
@@ -54,6 +57,17 @@ def _oracle_lib():
         lib.orc_orient.restype = ctypes.c_double
         lib.orc_insphere.argtypes = [c_double_p] * 5
         lib.orc_insphere.restype = ctypes.c_double
+        lib.orc_mesh_set_predicates.argtypes = [c_void_p, ctypes.c_int]
+        lib.orc_mesh_set_predicates.restype = ctypes.c_int
+        lib.orc_mesh_predicate_info.argtypes = [c_void_p, ctypes.POINTER(ctypes.c_long)]
+        lib.orc_mesh_predicate_info.restype = None
+        lib.orc_mesh_set_seed.argtypes = [c_void_p, ctypes.c_int]
+        lib.orc_mesh_set_seed.restype = ctypes.c_int
+        for name, n in (('orc_orient_exact_sign', 4), ('orc_insphere_exact_sign', 5),
+                        ('orc_orient_uncertain', 4), ('orc_insphere_uncertain', 5)):
+            fn = getattr(lib, name)
+            fn.argtypes = [c_double_p] * n
+            fn.restype = ctypes.c_int
         _olib = lib
     return _olib
 
@@ -90,6 +104,23 @@ class OracleMesh:
                                          _ip(self.tet_n), self.tet_v.shape[0])
         if not self._h:
             raise RuntimeError('orc_mesh_new failed')
+
+    def set_predicates(self, mode):
+        """'fast' (natinterp3d's signs), 'audit' (same signs, uncertain
+        evaluations counted) or 'exact'."""
+        if self._lib.orc_mesh_set_predicates(self._h, PREDICATE_MODES[mode]) != 0:
+            raise ValueError(mode)
+
+    def set_seed(self, first_tet):
+        """Walk seed: the nearest tet centroid (natinterp3d's k-d tree seed, the
+        default) or, with ``first_tet``, tet 0 (natinterp3d without its k-d tree)."""
+        self._lib.orc_mesh_set_seed(self._h, int(bool(first_tet)))
+
+    def predicate_info(self):
+        """(tets with an uncertain orientation sign, tets whose flag the exact sign flips)"""
+        out = (ctypes.c_long * 2)()
+        self._lib.orc_mesh_predicate_info(self._h, out)
+        return int(out[0]), int(out[1])
 
     def weights(self, queries_centered, with_stats=False):
         """CSR of Sibson weights (natinterp3d row/column order) for centred queries."""
@@ -155,6 +186,31 @@ def insphere(a, b, c, d, e):
     return lib.orc_insphere(*[_dp(p) for p in arr])
 
 
+def _pts(*ps):
+    arr = [np.ascontiguousarray(p, np.float64) for p in ps]
+    return arr, [_dp(p) for p in arr]
+
+
+def orient_exact_sign(a, b, c, d):
+    keep, ptrs = _pts(a, b, c, d)
+    return _oracle_lib().orc_orient_exact_sign(*ptrs)
+
+
+def insphere_exact_sign(a, b, c, d, e):
+    keep, ptrs = _pts(a, b, c, d, e)
+    return _oracle_lib().orc_insphere_exact_sign(*ptrs)
+
+
+def orient_uncertain(a, b, c, d):
+    keep, ptrs = _pts(a, b, c, d)
+    return bool(_oracle_lib().orc_orient_uncertain(*ptrs))
+
+
+def insphere_uncertain(a, b, c, d, e):
+    keep, ptrs = _pts(a, b, c, d, e)
+    return bool(_oracle_lib().orc_insphere_uncertain(*ptrs))
+
+
 # --------------------------------------------------------------------------
 # natinterp3d's own code (oracle/_ref)
 # --------------------------------------------------------------------------
@@ -184,6 +240,11 @@ def _ref_lib():
         lib.ref_query.restype = ctypes.c_int
         lib.ref_free_buffer.argtypes = [c_void_p]
         lib.ref_free_buffer.restype = None
+        if hasattr(lib, 'ref_orient3d_robust'):
+            lib.ref_orient3d_robust.argtypes = [c_double_p] * 4
+            lib.ref_orient3d_robust.restype = ctypes.c_double
+            lib.ref_insphere_robust.argtypes = [c_double_p] * 5
+            lib.ref_insphere_robust.restype = ctypes.c_double
         _rlib = lib
     return _rlib
 
@@ -200,6 +261,17 @@ def ref_query(native_mesh_ptr, queries_centered, n_keys, nthreads=0):
     if rc != 0:
         raise OverflowError('Total number of nonzero weights exceeds int32 limit')
     return _take_csr(lib.ref_free_buffer, vals_p, cols_p, rowptr, M, n_keys)
+
+
+def ref_orient3d_robust(a, b, c, d):
+    """Shewchuk's adaptive exact orient3d as shipped (and never called) by natinterp3d."""
+    keep, ptrs = _pts(a, b, c, d)
+    return _ref_lib().ref_orient3d_robust(*ptrs)
+
+
+def ref_insphere_robust(a, b, c, d, e):
+    keep, ptrs = _pts(a, b, c, d, e)
+    return _ref_lib().ref_insphere_robust(*ptrs)
 
 
 class RefInterpolator:

@@ -10,6 +10,10 @@
  *   ref_free   -> freeMeshAndVertices            (natural.c:120-123)
  *   ref_query  -> getInsertionFreeWeights[Parallel]
  *                                                (natural_insertionfree.c:761-831, 836-940)
+ *   ref_orient3d_robust / ref_insphere_robust -> Shewchuk's adaptive exact
+ *                orient3d / insphere (predicates.c:2294, 4160), which
+ *                natinterp3d ships but never calls; they pin the product's
+ *                exact predicates
  * ref_query also accepts a mesh built by the product's constructor library
  * (same natinterp3d sources, same flags, hence the same struct layout), which
  * is how the checker runs natinterp3d's query on exactly the exported mesh.
@@ -47,4 +51,25 @@ REF_API int ref_query(void *m, const double *queries, int num_queries, int nthre
 
 REF_API void ref_free_buffer(void *p) {
     free(p);
+}
+
+static int ref_exact_ready = 0;
+
+/* the adaptive predicates need exactinit() once (predicates.c:646) */
+REF_API double ref_orient3d_robust(const double *a, const double *b, const double *c,
+                                   const double *d) {
+    if (!ref_exact_ready) {
+        exactinit();
+        ref_exact_ready = 1;
+    }
+    return orient3d((double *)a, (double *)b, (double *)c, (double *)d);
+}
+
+REF_API double ref_insphere_robust(const double *a, const double *b, const double *c,
+                                   const double *d, const double *e) {
+    if (!ref_exact_ready) {
+        exactinit();
+        ref_exact_ready = 1;
+    }
+    return insphere((double *)a, (double *)b, (double *)c, (double *)d, (double *)e);
 }
