@@ -12,7 +12,13 @@ exchanged.  The collectives here are setup and bookkeeping only:
   an all-gather of the per-rank non-zero counts turns its local row pointers
   into the global ones (the matrix is the row-wise concatenation);
 * :func:`sharded_interpolate` -- each rank's block of ``W @ values``,
-  optionally all-gathered into the full result.
+  optionally all-gathered into the full result;
+* :func:`allreduce_grad` -- identity in the forward pass, sum over ranks of the
+  gradient in the backward pass: wrapped around ``values`` before a
+  differentiable interpolation of each rank's query shard, every rank ends
+  with d loss / d values of the whole batch (d/dqueries stays per shard);
+* :func:`shard_problems` / :func:`sharded_batch_interpolate` -- independent
+  problems split over ranks by query count (no exchange on the data path).
 
 Works with any ``torch.distributed`` backend (NCCL between GPUs, gloo on CPU).
 """
@@ -20,7 +26,8 @@ import numpy as np
 import torch
 import torch.distributed as dist
 
-__all__ = ['broadcast_mesh', 'shard_bounds', 'sharded_weights', 'sharded_interpolate']
+__all__ = ['broadcast_mesh', 'shard_bounds', 'sharded_weights', 'sharded_interpolate',
+           'allreduce_grad', 'shard_problems', 'sharded_batch_interpolate']
 
 
 def _tensor_device(group):
@@ -113,3 +120,67 @@ def sharded_interpolate(queries, interp_fn, group=None, gather=False):
         a, b = shard_bounds(M, r, world)
         blocks.append(parts[r][:b - a])
     return 0, torch.cat(blocks)
+
+
+class _AllReduceGrad(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, x, group):
+        ctx.group = group
+        return x.view_as(x)
+
+    @staticmethod
+    def backward(ctx, g):
+        g = g.contiguous().clone()
+        dist.all_reduce(g, op=dist.ReduceOp.SUM, group=ctx.group)
+        return g, None
+
+
+def allreduce_grad(values, group=None):
+    """``values`` unchanged; its gradient is summed over the ranks of ``group``
+    (each rank differentiates its own query shard: d loss / d values is the
+    sum of the shards' W_r^T g_r)."""
+    return _AllReduceGrad.apply(values, group)
+
+
+def shard_problems(costs, world):
+    """Problem indices per rank, balanced by cost (e.g. query counts): the
+    costliest problem goes to the least loaded rank, ties to the lower rank;
+    each rank's list is in ascending problem order."""
+    costs = np.asarray(costs, np.float64)
+    load = np.zeros(int(world))
+    parts = [[] for _ in range(int(world))]
+    for p in sorted(range(len(costs)), key=lambda i: (-costs[i], i)):
+        r = int(np.argmin(load))
+        parts[r].append(p)
+        load[r] += costs[p]
+    return [sorted(x) for x in parts]
+
+
+def sharded_batch_interpolate(keys_list, queries_list, values_list, group=None, device=None,
+                              batch_factory=None, gather=True):
+    """Independent problems over the ranks of ``group``: each rank builds and
+    evaluates its share (``batch_factory(keys) -> object with
+    .interpolate(queries_list, values_list)``, by default a
+    :class:`~natinterp3d_b200.batch.BatchInterpolator`).  Returns
+    {problem index: result} for this rank's problems, or for all problems
+    when ``gather`` (an object all-gather of the host results)."""
+    rank, world = dist.get_rank(group), dist.get_world_size(group)
+    mine = shard_problems([len(q) for q in queries_list], world)[rank]
+    out = {}
+    if mine:
+        if batch_factory is None:
+            from .batch import BatchInterpolator
+
+            def batch_factory(keys):
+                return BatchInterpolator(keys, device=device)
+        b = batch_factory([keys_list[p] for p in mine])
+        res = b.interpolate([queries_list[p] for p in mine], [values_list[p] for p in mine])
+        out = {p: np.asarray(r) for p, r in zip(mine, res)}
+    if not gather:
+        return out
+    parts = [None] * world
+    dist.all_gather_object(parts, out, group=group)
+    full = {}
+    for d in parts:
+        full.update(d)
+    return full
