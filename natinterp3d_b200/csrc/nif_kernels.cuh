@@ -178,7 +178,7 @@ struct Workspace {
     int nbr_vid[NBR_];
     int vh_key[VH_];
     int vh_first[VH_];
-    CavT cav_nbr[4 * CAV_];      // cavity index of neighbour f of cavity tet c, -1 outside
+    alignas(4) CavT cav_nbr[4 * CAV_];  // cavity index of neighbour f of cavity tet c, -1 outside
     CavT order[CAV_];            // cavity tets in natinterp3d's visiting order
     CavT pos[CAV_];              // inverse of order
     uint16_t bface[BF_];         // (cavity index << 2) | face
@@ -189,15 +189,18 @@ __device__ __forceinline__ unsigned mix_hash(int key) {
     return (unsigned)key * 2654435761u;
 }
 
-// Inserts key; returns its slot if newly inserted, -1 if already present.
-// Sets full when every slot was probed.
-__device__ __forceinline__ int hash_insert(int *keys, int hs, int key, bool &full) {
+// Inserts key; returns its slot, whether newly inserted (fresh = true) or
+// already present.  Returns -1 and sets full when every slot was probed.
+__device__ __forceinline__ int hash_insert(int *keys, int hs, int key, bool &fresh, bool &full) {
     unsigned h = mix_hash(key) & (unsigned)(hs - 1);
 #pragma unroll 1
     for (int probe = 0; probe < hs; ++probe) {
         const int old = atomicCAS(&keys[h], -1, key);
-        if (old == -1) return (int)h;
-        if (old == key) return -1;
+        if (old == -1) {
+            fresh = true;
+            return (int)h;
+        }
+        if (old == key) return (int)h;
         h = (h + 1) & (unsigned)(hs - 1);
     }
     full = true;
@@ -442,16 +445,28 @@ __device__ RowInfo sibson_row(const MeshView &M, const dv3 q, W &ws, const Grp<G
     const int start = t;
 
     // ---- 2. cavity: parallel flood over the tested-tet hash ----------------
+    // While a cavity tet's four neighbours are inserted into the hash, the
+    // slot of each is kept in nsl[4c+f] (aliasing cav_nbr, which is filled
+    // from it after the flood).  A missing neighbour (hull face of the
+    // super-simplex) gets the slot of the key NO_TET, inserted up front with
+    // hval = -1 and never queued, so every face has a slot.
+    static_assert(sizeof(slot_t) == sizeof(cav_t), "nsl aliases cav_nbr");
+    constexpr int NO_TET = -2;
+    slot_t *nsl = reinterpret_cast<slot_t *>(ws.cav_nbr);
     for (int i = g.lane; i < W::HS; i += G) {
         ws.u.a.hkey[i] = -1;
         ws.u.a.hval[i] = (cav_t)-1;
     }
     g.sync();
+    int none_slot = 0;
     if (g.lane == 0) {
         const int h = (int)(mix_hash(start) & (unsigned)(W::HS - 1));
         ws.u.a.hkey[h] = start;
         ws.u.a.queue[0] = (slot_t)h;
+        bool fresh = false, full = false;
+        none_slot = hash_insert(ws.u.a.hkey, W::HS, NO_TET, fresh, full);
     }
+    none_slot = g.shfl(none_slot, 0);
     g.sync();
     int qhead = 0, qtail = 1, ncav = 0;
     bool overflow = false;
@@ -512,10 +527,13 @@ __device__ RowInfo sibson_row(const MeshView &M, const dv3 q, W &ws, const Grp<G
         for (int k0 = 0; k0 < 4 * nnew; k0 += G) {
             const int k = k0 + g.lane;
             int ns = -1;
-            bool full = false;
+            bool full = false, fresh = false;
             if (k < 4 * nnew) {
                 const int nb = comp(M.tn[ws.cav_tet[base + (k >> 2)]], k & 3);
-                if (nb >= 0) ns = hash_insert(ws.u.a.hkey, W::HS, nb, full);
+                int sl = none_slot;
+                if (nb >= 0) sl = hash_insert(ws.u.a.hkey, W::HS, nb, fresh, full);
+                if (fresh) ns = sl;
+                nsl[4 * base + k] = (slot_t)(full ? none_slot : sl);
             }
             const unsigned pm = g.ballot(ns >= 0);
             const int qi = qtail + __popc(pm & g.lt());
@@ -555,15 +573,8 @@ __device__ RowInfo sibson_row(const MeshView &M, const dv3 q, W &ws, const Grp<G
     }
 
     // cavity-local neighbour table: cav_nbr[4c+f] = cavity index of s[f] or -1
-    for (int k = g.lane; k < 4 * ncav; k += G) {
-        const int nb = comp(M.tn[ws.cav_tet[k >> 2]], k & 3);
-        int v = -1;
-        if (nb >= 0) {
-            const int s = hash_find(ws.u.a.hkey, W::HS, nb);
-            v = (s >= 0) ? (int)ws.u.a.hval[s] : -1;
-        }
-        ws.cav_nbr[k] = (cav_t)v;
-    }
+    // (every neighbour slot recorded by the flood has been tested by now)
+    for (int k = g.lane; k < 4 * ncav; k += G) ws.cav_nbr[k] = ws.u.a.hval[nsl[k]];
     for (int c = g.lane; c < ncav; c += G) ws.pos[c] = (cav_t)-1;
     g.sync();
 
@@ -587,8 +598,18 @@ __device__ RowInfo sibson_row(const MeshView &M, const dv3 q, W &ws, const Grp<G
                 const uint64_t bit = 1ull << (c & 63);
                 if ((c < 64 ? v0 : v1) & bit) continue;
                 if (c < 64) v0 |= bit; else v1 |= bit;
-                const int n0 = ws.cav_nbr[4 * c], n1 = ws.cav_nbr[4 * c + 1];
-                const int n2 = ws.cav_nbr[4 * c + 2], n3 = ws.cav_nbr[4 * c + 3];
+                int n0, n1, n2, n3;
+                if constexpr (sizeof(cav_t) == 1) {
+                    // the four signed 8-bit entries of tet c in one 32-bit load
+                    const int w = *reinterpret_cast<const int *>(&ws.cav_nbr[4 * c]);
+                    n0 = (int8_t)(w & 0xff);
+                    n1 = (int8_t)((w >> 8) & 0xff);
+                    n2 = (int8_t)((w >> 16) & 0xff);
+                    n3 = (int8_t)((unsigned)w >> 24);
+                } else {
+                    n0 = ws.cav_nbr[4 * c], n1 = ws.cav_nbr[4 * c + 1];
+                    n2 = ws.cav_nbr[4 * c + 2], n3 = ws.cav_nbr[4 * c + 3];
+                }
                 ws.pos[c] = (cav_t)nord;
                 ws.order[nord++] = (cav_t)c;
                 const int nb[4] = {n0, n1, n2, n3};
