@@ -63,7 +63,20 @@ def parse():
                         'batched: 512 uneven problems (keys log-uniform [500, 100k], queries '
                         'log-uniform [1k, 200k], boxes of side 0.5-2, D=4 float32, seed 4)')
     p.add_argument('--problems', type=int, default=512)
+    p.add_argument('--no-tune', action='store_true',
+                   help="skip the autotuner (untimed setup) and keep the library's default "
+                        "launch settings")
+    p.add_argument('--tuning', default=None,
+                   help='fixed launch settings blocks_per_sm,bucket_shift,tile (e.g. 8,0,8) '
+                        'instead of the autotuner')
     return p.parse_args()
+
+
+def fixed_tuning(args):
+    if not args.tuning:
+        return None
+    b, s, t = (int(x) for x in args.tuning.split(','))
+    return {'blocks_per_sm': b, 'bucket_shift': s, 'tile': t}
 
 
 def make_data(args, rank=0):
@@ -253,6 +266,12 @@ def run_fwdbwd(args, rank, world, local_rank):
     qd = torch.from_numpy(rng.uniform(0.1, 0.9, (q_n, 3))).to(dev)
     vd = torch.from_numpy(rng.standard_normal((keys_n, dim)).astype(np.float32)).to(dev)
     gd = torch.from_numpy(rng.standard_normal((q_n, dim))).to(dev)
+    # autotuner (setup, untimed) on the weights path the differentiable forward uses
+    tuned = None
+    if fixed_tuning(args):
+        interp.set_tuning(fixed_tuning(args))
+    elif not args.no_tune:
+        tuned = interp.tune(qd, mode='weights', use_cache=False)['tuning']
 
     def fwd():
         return interp.interpolate_device(qd, vd, check=False)
@@ -286,7 +305,8 @@ def run_fwdbwd(args, rank, world, local_rank):
             'higher_is_better': True, 'dtype': 'f64', 'data': 'synthetic',
             'config': {'workload': 'differentiable: %d keys U[0,1]^3, %d queries U[0.1,0.9]^3 float64 '
                                    'with grad, values D=%d float32 with grad, loss=sum(out*g), seed 3'
-                                   % (keys_n, q_n, dim)}}))
+                                   % (keys_n, q_n, dim),
+                       'tuning': interp.tuning, 'autotuned': tuned is not None}}))
 
 
 def batched_workload(P, seed):
@@ -318,6 +338,12 @@ def run_batched(args, rank, world, local_rank):
     M = int(qoff[-1])
     qcat = torch.from_numpy(np.concatenate(queries)).to(dev)
     vcat = torch.from_numpy(np.concatenate(values)).to(dev)
+    # autotuner (setup, untimed): occupancy and tile size of the persistent kernel
+    tuned = None
+    if fixed_tuning(args):
+        b.set_tuning(fixed_tuning(args))
+    elif not args.no_tune:
+        tuned = b.tune(qcat, qoff, vcat, use_cache=False)['tuning']
     graph = b.capture(qcat, qoff, vcat)
     eager = b.interpolate_per_problem(qcat, qoff, vcat)
     same = bool(torch.equal(graph.replay(), eager))
@@ -371,7 +397,8 @@ def run_batched(args, rank, world, local_rank):
                                    'queries log-uniform [1k, 200k] in the boxes shrunk 5%%, values D=4 '
                                    'float32, seed 4' % args.problems,
                        'total_keys': int(b.n_keys.sum()), 'total_queries': M,
-                       'mesh_build_s': round(build_s, 1)}}))
+                       'mesh_build_s': round(build_s, 1), 'tuning': b.get_tuning(),
+                       'autotuned': tuned is not None}}))
 
 
 def main():
@@ -425,6 +452,16 @@ def main():
     Wref, stats, _ = om.weights(queries[:sample_n] - interp.centroid, with_stats=True)
     out_s = dm.interpolate(qd[:sample_n], vd, interp.centroid).cpu().numpy()
     exact = bool(np.array_equal(out_s, Wref @ values))
+
+    # autotuner (setup, untimed): launch settings for this workload, timed on
+    # a 2M-query sample; results do not depend on them
+    t0 = time.perf_counter()
+    tuned = None
+    if fixed_tuning(args):
+        interp.set_tuning(fixed_tuning(args))
+    elif not args.no_tune:
+        tuned = interp.tune(qd, vd, use_cache=False)['tuning']
+    tune_s = time.perf_counter() - t0
 
     def step():
         return dm.interpolate(qd, vd, interp.centroid, check=False)
@@ -495,6 +532,8 @@ def main():
                 'mesh_build_s': round(build_s, 2), 'mesh_upload_s': round(upload_s, 3),
                 'tets': dm.n_tets, 'bit_identical_to_oracle_on_sample': exact,
                 'predicates': args.predicates,
+                'tuning': dm.get_tuning(), 'autotuned': tuned is not None,
+                'tune_s': round(tune_s, 2),
             },
             'roofline': {
                 'bound': 'fp64', 'kernel': 'k_rows_fast',

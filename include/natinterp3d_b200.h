@@ -133,6 +133,34 @@ int nif_dmesh_info(const nif_dmesh *m, int64_t info[8]);
 #define NIF_PRED_EXACT 2
 int nif_dmesh_set_predicates(nif_dmesh *m, int mode);
 
+/* Launch settings of the query kernels.  They change speed, never results:
+ * every setting gives bit-identical output.  (No counterpart in natinterp3d,
+ * whose query loop is OpenMP `schedule(dynamic, 64)` over Morton-sorted
+ * queries, natural_insertionfree.c:856, 866-887.)
+ *   blocks_per_sm  resident 4-warp blocks per SM of the shared-memory row
+ *                  kernel, one warp per query: 6 (80 registers a thread) or
+ *                  8 (64 registers, more spills, more warps hiding latency)
+ *   bucket_shift   Morton bucket resolution of the query ordering, in bits per
+ *                  axis relative to the size-based default: -2 .. 1
+ *   tile           queries a warp takes per work item: 0 = a static grid
+ *                  stride (one query per step), 1 .. 1024 = tiles of
+ *                  consecutive bucket-ordered queries pulled from a device
+ *                  counter
+ * nif_dmesh_set_tuning applies to later query calls on the mesh (the
+ * workspace size depends on bucket_shift: query nif_query_workspace_bytes
+ * after setting it); nif_batch_set_tuning to later batch calls, which ignore
+ * bucket_shift and need tile >= 1.  nif_interpolate_noalloc uses only
+ * blocks_per_sm.  Defaults: {8, 0, 0} for a mesh, {8, 0, 64} for a batch.
+ * Out-of-range values return NIF_ERR_ARG and change nothing. */
+typedef struct {
+    int32_t blocks_per_sm;
+    int32_t bucket_shift;
+    int32_t tile;
+    int32_t reserved; /* 0 */
+} nif_tuning;
+int nif_dmesh_set_tuning(nif_dmesh *m, const nif_tuning *t);
+int nif_dmesh_get_tuning(const nif_dmesh *m, nif_tuning *t);
+
 /* Result summary of one query call (host memory). */
 typedef struct {
     int64_t nnz;            /* non-zeros of the weight matrix */
@@ -242,6 +270,9 @@ int nif_batch_create(int n_problems, nif_dmesh *const *meshes, void *d_buf, size
                      void *stream, nif_dbatch **out);
 void nif_batch_destroy(nif_dbatch *b);
 int nif_batch_workspace_bytes(const nif_dbatch *b, int64_t total_queries, size_t *bytes);
+/* Launch settings of later batch calls (nif_tuning above). */
+int nif_batch_set_tuning(nif_dbatch *b, const nif_tuning *t);
+int nif_batch_get_tuning(const nif_dbatch *b, nif_tuning *t);
 
 /* Interpolation of every problem at once.  Queries [sum M_p][3] and values
  * [sum N_p][D] are concatenated by problem; d_query_offsets and
@@ -251,7 +282,8 @@ int nif_batch_workspace_bytes(const nif_dbatch *b, int64_t total_queries, size_t
  * The call makes no host synchronisation and reads nothing from the host,
  * so a stream capture of it replays as one CUDA graph: bucketing by
  * (problem, Morton cell), one persistent row kernel whose warps take tiles
- * of 64 queries from a device work counter, then the large-row kernel.
+ * of queries (64 by default, nif_batch_set_tuning) from a device work
+ * counter, then the large-row kernel.
  * Read the row counters afterwards with nif_batch_summary. */
 int nif_batch_interpolate(const nif_dbatch *b, const void *d_queries, int query_dtype,
                           const int64_t *d_query_offsets, const double *d_centroids,

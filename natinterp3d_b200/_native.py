@@ -168,6 +168,20 @@ class Summary(ctypes.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_ if k != 'reserved'}
 
 
+class Tuning(ctypes.Structure):
+    """nif_tuning: launch settings of the query kernels (speed only, never results)."""
+    _fields_ = [('blocks_per_sm', ctypes.c_int32), ('bucket_shift', ctypes.c_int32),
+                ('tile', ctypes.c_int32), ('reserved', ctypes.c_int32)]
+
+    def as_dict(self):
+        return {'blocks_per_sm': self.blocks_per_sm, 'bucket_shift': self.bucket_shift,
+                'tile': self.tile}
+
+    @classmethod
+    def from_dict(cls, d):
+        return cls(int(d['blocks_per_sm']), int(d.get('bucket_shift', 0)), int(d.get('tile', 0)), 0)
+
+
 # every symbol include/natinterp3d_b200.h declares for libnif_cuda.so, with its ctypes signature
 CUDA_SIGNATURES = {
     'nif_dmesh_bytes': (c_int, [c_int, c_int, ctypes.POINTER(c_size_t)]),
@@ -176,6 +190,8 @@ CUDA_SIGNATURES = {
     'nif_dmesh_destroy': (None, [c_void_p]),
     'nif_dmesh_info': (c_int, [c_void_p, ctypes.POINTER(c_int64)]),
     'nif_dmesh_set_predicates': (c_int, [c_void_p, c_int]),
+    'nif_dmesh_set_tuning': (c_int, [c_void_p, ctypes.POINTER(Tuning)]),
+    'nif_dmesh_get_tuning': (c_int, [c_void_p, ctypes.POINTER(Tuning)]),
     'nif_query_workspace_bytes': (c_int, [c_void_p, c_int64, c_int, ctypes.POINTER(c_size_t)]),
     'nif_weights_count': (c_int, [c_void_p, c_void_p, c_int, c_int64, c_double_p, c_void_p,
                                   c_size_t, c_void_p, c_void_p, ctypes.POINTER(Summary)]),
@@ -202,6 +218,8 @@ CUDA_SIGNATURES = {
                                  ctypes.POINTER(c_void_p)]),
     'nif_batch_destroy': (None, [c_void_p]),
     'nif_batch_workspace_bytes': (c_int, [c_void_p, c_int64, ctypes.POINTER(c_size_t)]),
+    'nif_batch_set_tuning': (c_int, [c_void_p, ctypes.POINTER(Tuning)]),
+    'nif_batch_get_tuning': (c_int, [c_void_p, ctypes.POINTER(Tuning)]),
     'nif_batch_interpolate': (c_int, [c_void_p, c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_int,
                                       c_void_p, c_int, c_void_p, c_int, c_int64, c_void_p, c_size_t,
                                       c_void_p]),

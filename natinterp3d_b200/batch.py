@@ -61,6 +61,28 @@ class BatchInterpolator:
             cens = np.stack([it.centroid for it in self.interpolators])
             self.centroids = torch.from_numpy(np.ascontiguousarray(cens)).to(self.device)
 
+    # ------------------------------------------------------------------ tuning
+    def set_tuning(self, tuning):
+        """Launch settings of later batch calls (``blocks_per_sm`` 6 or 8,
+        ``tile`` 1..1024 queries per work item; ``bucket_shift`` is ignored).
+        A graph captured earlier keeps the settings it was captured with."""
+        t = N.Tuning.from_dict(tuning)
+        rc = self._lib.nif_batch_set_tuning(self._h, ctypes.byref(t))
+        if rc == N.NIF_ERR_ARG:
+            raise ValueError('invalid batch tuning %r' % (tuning,))
+        N.check(rc, 'nif_batch_set_tuning')
+
+    def get_tuning(self):
+        t = N.Tuning()
+        N.check(self._lib.nif_batch_get_tuning(self._h, ctypes.byref(t)), 'nif_batch_get_tuning')
+        return t.as_dict()
+
+    def tune(self, queries, query_offsets, values, **kw):
+        """Time the candidate launch settings on these inputs and keep the
+        fastest (:func:`natinterp3d_b200.tuning.tune_batch`)."""
+        from .tuning import tune_batch
+        return tune_batch(self, queries, query_offsets, values, **kw)
+
     # ------------------------------------------------------------------ helpers
     def query_offsets(self, counts):
         off = np.zeros(self.P + 1, np.int64)

@@ -40,9 +40,13 @@ namespace nif {
 #ifndef NIF_FAST_G
 #define NIF_FAST_G 32
 #endif
-#ifndef NIF_FAST_MINB
-#define NIF_FAST_MINB 6
-#endif
+// resident 4-warp blocks per SM of the shared-memory row kernels: the two
+// occupancy points compiled (nif_tuning.blocks_per_sm) and the default
+constexpr int OCC_LO = 6;   // 80 registers a thread
+constexpr int OCC_HI = 8;   // 64 registers a thread
+constexpr int OCC_DEFAULT = OCC_HI;
+constexpr int TILE_MAX = 1024;
+constexpr int BATCH_TILE_DEFAULT = 64;
 constexpr int FAST_G = NIF_FAST_G;    // lanes per query in the shared-memory kernel
 using FastWS = Workspace<256, 96, 128, 64, 128, FAST_G, uint8_t, int8_t>;
 constexpr int LARGE_G = 32;
@@ -380,7 +384,6 @@ __global__ void k_scan_apply(const int *__restrict__ in, int64_t n, const OutT *
 // get_weights: rows staged per original row index, compacted afterwards
 struct StageSink {
     static constexpr bool FULL = true;
-    static constexpr int MIN_BLOCKS = NIF_FAST_MINB;
     int *__restrict__ cnt;          // [M]
     int64_t *__restrict__ src;      // [M] first staged entry of the row
     int *__restrict__ cols;         // [M*ROW_CAP + arena]
@@ -448,7 +451,6 @@ struct InterpSink {
     CT *__restrict__ out;           // [M][D]
     int D;
     static constexpr bool FULL = true;
-    static constexpr int MIN_BLOCKS = NIF_FAST_MINB;
     static constexpr bool SORTED = sizeof(WT) == 4;
 
     template <int G, class W>
@@ -760,21 +762,35 @@ __device__ __forceinline__ void record(DevSummary *sum, const RowInfo &r, int la
 }
 
 // fast path: shared-memory scratch, rows in bucket order; PM is PM_PLAIN or
-// PM_FILTER
-template <class QT, class Sink, int PM>
-__global__ void __launch_bounds__(FAST_BLOCK, Sink::MIN_BLOCKS) k_rows_fast(MeshView M, const QT *__restrict__ Q,
+// PM_FILTER; OCC resident blocks per SM.  With tile == 0 group k takes rows
+// k, k + ng, k + 2 ng, ...; with tile > 0 it takes tiles of `tile`
+// consecutive rows from the device counter (zeroed before the launch).
+template <class QT, class Sink, int PM, int OCC>
+__global__ void __launch_bounds__(FAST_BLOCK, OCC) k_rows_fast(MeshView M, const QT *__restrict__ Q,
                                                           Centroid cen, const int *__restrict__ order,
                                                           int64_t nrows, Sink sink, LargeQueue lq,
-                                                          DevSummary *sum) {
+                                                          DevSummary *sum, int tile,
+                                                          unsigned long long *counter) {
     extern __shared__ __align__(16) unsigned char smem[];
     constexpr int G = FAST_G;
     constexpr int GPB = FAST_BLOCK / G;
     Grp<G> g;
     FastWS &ws = reinterpret_cast<FastWS *>(smem)[threadIdx.x / G];
-    const int64_t gid = (int64_t)blockIdx.x * GPB + threadIdx.x / G;
+    const int64_t gid = tile <= 0 ? (int64_t)blockIdx.x * GPB + threadIdx.x / G : 0;
     const int64_t ng = (int64_t)gridDim.x * GPB;
     unsigned long long steps = 0;
-    for (int64_t s = gid; s < nrows; s += ng) {
+    // one loop for both schedules, so that the row routine is inlined once
+    int64_t s = gid, s1 = tile <= 0 ? nrows : 0;  // tiled: fetch a tile first
+    for (;;) {
+        if (s >= s1) {
+            if (tile <= 0) break;
+            unsigned long long t = 0;
+            if (g.lane == 0) t = atomicAdd(counter, 1ull);
+            t = __shfl_sync(g.mask, t, 0, G);
+            s = (int64_t)t * tile;
+            if (s >= nrows) break;
+            s1 = min(nrows, s + (int64_t)tile);
+        }
         const int64_t i = order[s];
         const dv3 q = load_query(Q, i, cen.c);
         const RowInfo r = sibson_row<G, FastWS, Sink::FULL, PM>(M, q, ws, g);
@@ -793,6 +809,7 @@ __global__ void __launch_bounds__(FAST_BLOCK, Sink::MIN_BLOCKS) k_rows_fast(Mesh
             sink.template emit<G>(i, r.status == ST_OK ? r.nnb : 0, ws, g, false, M, q, r);
         }
         g.sync();
+        s += tile <= 0 ? ng : 1;
     }
     if (g.lane == 0 && steps) atomicAdd(&sum->walk_steps, steps);
 }
@@ -899,6 +916,7 @@ struct nif_dmesh {
     int num_sms;
     size_t bytes;
     int64_t orient_unc, orient_flip;  // tets with an uncertain / flipped orientation flag
+    nif_tuning tune{OCC_DEFAULT, 0, 0, 0};
 };
 
 namespace {
@@ -971,6 +989,8 @@ int blocks_for(int64_t n, int threads, int cap = 148 * 32) {
 // query workspace layout
 struct QueryLayout {
     DevSummary *sum;
+    unsigned long long *counter;  // work-item counter of the tiled row schedule
+    int bits_cap;                 // largest bucket resolution bcount holds (bits per axis)
     int *bucket, *bcount, *order, *large_list;
     int64_t *scan_bsum;     // block sums for the scans
     int64_t *scan_total;
@@ -991,12 +1011,16 @@ int bucket_bits(int64_t M) {
     return b;
 }
 
+// The layout does not depend on the mesh's tuning: bcount has room for one
+// bucket bit per axis more than the default, and run_bucketing clamps to it.
 QueryLayout carve_query(Carve &c, int64_t M, int mode) {
     QueryLayout L{};
-    const int bits = bucket_bits(M);
+    const int bits = min(10, bucket_bits(M) + 1);
     const int64_t nbk = (int64_t)1 << (3 * bits);
     const int64_t mscan = M > nbk ? M : nbk;
+    L.bits_cap = bits;
     L.sum = c.take<DevSummary>(1);
+    L.counter = c.take<unsigned long long>(1);
     L.bucket = c.take<int>(M > 0 ? M : 1);
     L.bcount = c.take<int>(nbk + 1);
     L.order = c.take<int>(M > 0 ? M : 1);
@@ -1061,7 +1085,7 @@ inline void prof_mark(int k, cudaStream_t st) {
 template <class QT>
 void run_bucketing(const nif_dmesh *m, const QT *Q, int64_t M, const Centroid &cen,
                    const QueryLayout &L, cudaStream_t st) {
-    const int bits = bucket_bits(M);
+    const int bits = max(1, min(L.bits_cap, bucket_bits(M) + m->tune.bucket_shift));
     const int64_t nbk = (int64_t)1 << (3 * bits);
     prof_mark(0, st);
     cudaMemsetAsync(L.bcount, 0, sizeof(int) * (nbk + 1), st);
@@ -1074,12 +1098,12 @@ void run_bucketing(const nif_dmesh *m, const QT *Q, int64_t M, const Centroid &c
 }
 
 // persistent grid of the fast row kernel: resident blocks per SM x SMs
-template <class QT, class Sink, int PM>
-void launch_fast(const nif_dmesh *m, const QT *Q, int64_t M, const Centroid &cen,
-                 const QueryLayout &L, const Sink &sink, cudaStream_t st) {
+template <class QT, class Sink, int PM, int OCC>
+void launch_fast_occ(const nif_dmesh *m, const QT *Q, int64_t M, const Centroid &cen,
+                     const QueryLayout &L, const Sink &sink, cudaStream_t st) {
     constexpr int GPB = FAST_BLOCK / FAST_G;
     const size_t smem = GPB * sizeof(FastWS);
-    auto kern = k_rows_fast<QT, Sink, PM>;
+    auto kern = k_rows_fast<QT, Sink, PM, OCC>;
     static int per_sm = -1;  // resident blocks per SM of this instantiation
     if (per_sm < 0) {
         if (smem > 48 * 1024) set_smem(kern, smem);
@@ -1087,12 +1111,28 @@ void launch_fast(const nif_dmesh *m, const QT *Q, int64_t M, const Centroid &cen
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, FAST_BLOCK, smem);
         if (per_sm < 1) per_sm = 1;
     }
+    const int tile = m->tune.tile;
     int64_t blocks = (M + GPB - 1) / GPB;
+    if (tile > 0) blocks = (M + (int64_t)GPB * tile - 1) / ((int64_t)GPB * tile);
     const int64_t cap = (int64_t)per_sm * m->num_sms;
     if (blocks > cap) blocks = cap;
     if (blocks < 1) blocks = 1;
+    if (tile > 0) cudaMemsetAsync(L.counter, 0, sizeof(unsigned long long), st);
     kern<<<(unsigned)blocks, FAST_BLOCK, smem, st>>>(m->view, Q, cen, L.order, M, sink,
-                                                    LargeQueue{L.large_list}, L.sum);
+                                                    LargeQueue{L.large_list}, L.sum, tile, L.counter);
+}
+
+// the structure-only (gradient) rows keep their own occupancy; the others
+// run at the mesh's tuned one
+template <class QT, class Sink, int PM>
+void launch_fast(const nif_dmesh *m, const QT *Q, int64_t M, const Centroid &cen,
+                 const QueryLayout &L, const Sink &sink, cudaStream_t st) {
+    if constexpr (!Sink::FULL)
+        launch_fast_occ<QT, Sink, PM, Sink::MIN_BLOCKS>(m, Q, M, cen, L, sink, st);
+    else if (m->tune.blocks_per_sm == OCC_LO)
+        launch_fast_occ<QT, Sink, PM, OCC_LO>(m, Q, M, cen, L, sink, st);
+    else
+        launch_fast_occ<QT, Sink, PM, OCC_HI>(m, Q, M, cen, L, sink, st);
 }
 
 // fast rows (filtered when the mesh's predicate mode is not the default),
@@ -1321,6 +1361,27 @@ NIF_EXPORT int nif_dmesh_set_predicates(nif_dmesh *m, int mode) {
     return NIF_OK;
 }
 
+namespace {
+// a tuning is valid for a mesh (batch = false) or a batch (batch = true)
+bool tuning_ok(const nif_tuning *t, bool batch) {
+    return t && (t->blocks_per_sm == OCC_LO || t->blocks_per_sm == OCC_HI) &&
+           t->bucket_shift >= -2 && t->bucket_shift <= 1 && t->tile >= (batch ? 1 : 0) &&
+           t->tile <= TILE_MAX && t->reserved == 0;
+}
+}  // namespace
+
+NIF_EXPORT int nif_dmesh_set_tuning(nif_dmesh *m, const nif_tuning *t) {
+    if (!m || !tuning_ok(t, false)) return NIF_ERR_ARG;
+    m->tune = *t;
+    return NIF_OK;
+}
+
+NIF_EXPORT int nif_dmesh_get_tuning(const nif_dmesh *m, nif_tuning *t) {
+    if (!m || !t) return NIF_ERR_ARG;
+    *t = m->tune;
+    return NIF_OK;
+}
+
 NIF_EXPORT int nif_query_workspace_bytes(const nif_dmesh *m, int64_t M, int mode, size_t *bytes) {
     if (!m || !bytes || M < 0 || (mode != NIF_MODE_WEIGHTS && mode != NIF_MODE_INTERP))
         return NIF_ERR_ARG;
@@ -1530,7 +1591,9 @@ QueryLayout carve_noalloc(Carve &c, int64_t M) {
     const int bits = bucket_bits(M);
     const int64_t nbk = (int64_t)1 << (3 * bits);
     const int64_t mscan = M > nbk ? M : nbk;
+    L.bits_cap = bits;  // a positive bucket_shift is capped at the default here
     L.sum = c.take<DevSummary>(1);
+    L.counter = c.take<unsigned long long>(1);
     L.bucket = c.take<int>(M > 0 ? M : 1);
     L.bcount = c.take<int>(nbk + 1);
     L.order = c.take<int>(M > 0 ? M : 1);
@@ -1776,7 +1839,6 @@ NIF_EXPORT int nif_query_grad(const nif_dmesh *m, const void *d_queries, int que
 // ===========================================================================
 namespace nif {
 
-constexpr int BATCH_TILE = 64;  // queries per work item of the persistent kernel
 
 __device__ __forceinline__ int find_problem(const int64_t *__restrict__ off, int P, int64_t i) {
     int lo = 0, hi = P;  // off[lo] <= i < off[hi]
@@ -1836,7 +1898,6 @@ __global__ void k_batch_bucket(const QT *__restrict__ Q, int64_t M, const int64_
 template <class WT, class VT, class CT>
 struct BatchInterpSink {
     static constexpr bool FULL = true;
-    static constexpr int MIN_BLOCKS = NIF_FAST_MINB;
     const VT *__restrict__ values;   // concatenated [sum N_p][D]
     const int64_t *__restrict__ koff; // [P+1] key offsets
     const int64_t *__restrict__ qoff; // [P+1] query offsets
@@ -1856,12 +1917,12 @@ struct BatchInterpSink {
 // persistent row kernel of a batch: warps pull tiles of bucket-ordered
 // queries from a device counter; the mesh view of the current problem is
 // kept in shared memory
-template <class QT, class Sink, int PM>
-__global__ void __launch_bounds__(FAST_BLOCK, Sink::MIN_BLOCKS)
+template <class QT, class Sink, int PM, int OCC>
+__global__ void __launch_bounds__(FAST_BLOCK, OCC)
     k_rows_batch(const MeshView *__restrict__ views, const int64_t *__restrict__ qoff, int P,
                  const QT *__restrict__ Q, const double *__restrict__ cens,
                  const int *__restrict__ order, int64_t nrows, Sink sink, LargeQueue lq,
-                 DevSummary *sum, unsigned long long *counter) {
+                 DevSummary *sum, unsigned long long *counter, int tile) {
     extern __shared__ __align__(16) unsigned char smem[];
     constexpr int G = FAST_G;
     constexpr int GPB = FAST_BLOCK / G;
@@ -1873,12 +1934,12 @@ __global__ void __launch_bounds__(FAST_BLOCK, Sink::MIN_BLOCKS)
     int cur = -1;
     unsigned long long steps = 0;
     for (;;) {
-        unsigned long long tile = 0;
-        if (g.lane == 0) tile = atomicAdd(counter, 1ull);
-        tile = __shfl_sync(g.mask, tile, 0, G);
-        const int64_t s0 = (int64_t)tile * BATCH_TILE;
+        unsigned long long t = 0;
+        if (g.lane == 0) t = atomicAdd(counter, 1ull);
+        t = __shfl_sync(g.mask, t, 0, G);
+        const int64_t s0 = (int64_t)t * tile;
         if (s0 >= nrows) break;
-        const int64_t s1 = min(nrows, s0 + BATCH_TILE);
+        const int64_t s1 = min(nrows, s0 + (int64_t)tile);
         for (int64_t s = s0; s < s1; s++) {
             const int64_t i = order[s];
             const int p = find_problem(qoff, P, i);
@@ -1958,6 +2019,7 @@ struct nif_dbatch {
     int num_sms;
     bool filtered;      // some mesh uses a non-default predicate mode
     MeshView *d_views;  // [P] in the caller's buffer
+    nif_tuning tune{OCC_DEFAULT, 0, BATCH_TILE_DEFAULT, 0};
 };
 
 namespace {
@@ -1989,12 +2051,13 @@ BatchLayout carve_batch(Carve &c, int P, int64_t M) {
     return L;
 }
 
-template <class QT, class Sink, int PM>
-void launch_batch_rows(const nif_dbatch *b, const QT *Q, int64_t M, const int64_t *qoff,
-                       const double *cens, const Sink &sink, const BatchLayout &L, cudaStream_t st) {
+template <class QT, class Sink, int PM, int OCC>
+void launch_batch_rows_occ(const nif_dbatch *b, const QT *Q, int64_t M, const int64_t *qoff,
+                           const double *cens, const Sink &sink, const BatchLayout &L,
+                           cudaStream_t st) {
     constexpr int GPB = FAST_BLOCK / FAST_G;
     const size_t smem = GPB * sizeof(FastWS);
-    auto kern = k_rows_batch<QT, Sink, PM>;
+    auto kern = k_rows_batch<QT, Sink, PM, OCC>;
     static int per_sm = -1;
     if (per_sm < 0) {
         if (smem > 40 * 1024) set_smem(kern, smem);
@@ -2002,12 +2065,22 @@ void launch_batch_rows(const nif_dbatch *b, const QT *Q, int64_t M, const int64_
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, FAST_BLOCK, smem);
         if (per_sm < 1) per_sm = 1;
     }
-    const int64_t want = (M + (int64_t)GPB * BATCH_TILE - 1) / ((int64_t)GPB * BATCH_TILE);
+    const int tile = b->tune.tile;
+    const int64_t want = (M + (int64_t)GPB * tile - 1) / ((int64_t)GPB * tile);
     int64_t blocks = (int64_t)per_sm * b->num_sms;
     if (blocks > want) blocks = want;
     if (blocks < 1) blocks = 1;
     kern<<<(unsigned)blocks, FAST_BLOCK, smem, st>>>(b->d_views, qoff, b->P, Q, cens, L.order, M, sink,
-                                                    LargeQueue{L.large_list}, L.sum, L.counter);
+                                                    LargeQueue{L.large_list}, L.sum, L.counter, tile);
+}
+
+template <class QT, class Sink, int PM>
+void launch_batch_rows(const nif_dbatch *b, const QT *Q, int64_t M, const int64_t *qoff,
+                       const double *cens, const Sink &sink, const BatchLayout &L, cudaStream_t st) {
+    if (b->tune.blocks_per_sm == OCC_LO)
+        launch_batch_rows_occ<QT, Sink, PM, OCC_LO>(b, Q, M, qoff, cens, sink, L, st);
+    else
+        launch_batch_rows_occ<QT, Sink, PM, OCC_HI>(b, Q, M, qoff, cens, sink, L, st);
 }
 
 template <class QT, class VT, class CT>
@@ -2036,6 +2109,18 @@ void batch_typed(const nif_dbatch *b, const void *q, int64_t M, const int64_t *q
 }
 
 }  // namespace
+
+NIF_EXPORT int nif_batch_set_tuning(nif_dbatch *b, const nif_tuning *t) {
+    if (!b || !tuning_ok(t, true)) return NIF_ERR_ARG;
+    b->tune = *t;
+    return NIF_OK;
+}
+
+NIF_EXPORT int nif_batch_get_tuning(const nif_dbatch *b, nif_tuning *t) {
+    if (!b || !t) return NIF_ERR_ARG;
+    *t = b->tune;
+    return NIF_OK;
+}
 
 NIF_EXPORT int nif_batch_bytes(int n_problems, size_t *bytes) {
     if (!bytes || n_problems < 1) return NIF_ERR_ARG;

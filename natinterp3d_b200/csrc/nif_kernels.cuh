@@ -397,6 +397,7 @@ __device__ RowInfo sibson_row(const MeshView &M, const dv3 q, W &ws, const Grp<G
         }
         ++r.steps;
         const int4 p = M.tv[t];
+        const int4 nbs = M.tn[t];  // loaded with p: no second dependent trip per step
         int sg = 1;
         bool unc = false;
         dv3 v1{0.0, 0.0, 0.0}, v2 = v1, v3 = v1;
@@ -435,7 +436,7 @@ __device__ RowInfo sibson_row(const MeshView &M, const dv3 q, W &ws, const Grp<G
             }
         }
         if (!m) break;
-        const int nb = comp(M.tn[t], __ffs(m) - 1);
+        const int nb = comp(nbs, __ffs(m) - 1);
         if (nb < 0) {
             r.outside = true;
             return r;
@@ -714,46 +715,99 @@ __device__ RowInfo sibson_row(const MeshView &M, const dv3 q, W &ws, const Grp<G
 
     // ---- 4. stolen volumes ----------------------------------------------------
     // Items in natinterp3d's order: the 4 vertices of every cavity tet (cavity
-    // order), then the 3 vertices of every boundary face (face order).  Each
-    // lane computes one item's signed subcell volume; lanes whose items belong
-    // to the same neighbour are folded into acc[] by the lowest of them, in
-    // lane order, so every acc[] is a left-to-right sum in item order.
-    const int n_old = 4 * ncav;
-    const int n_all = n_old + 3 * nbf;
-    for (int k0 = 0; k0 < n_all; k0 += G) {
-        const int k = k0 + g.lane;
-        int s = -1;
-        double term = 0.0;
-        if (k < n_all) {
-            dv3 pk, pa, pb, pc, ct, f1, f2, f3;
-            bool old_term = k < n_old;
-            if (old_term) {
-                // cavity tet c, vertex vi (natural_insertionfree.c:642-676)
-                const int c = ws.order[k >> 2];
-                const int vi = k & 3;
+    // order), then the 3 vertices of every boundary face (face order).  One
+    // lane computes the items of one cavity tet (4) or one boundary face (3),
+    // sharing that tet's loads and face-circumcentre choices, or the face's
+    // virtual-tet circumcentre, among them; the terms go to a shared buffer
+    // in item order.  Then lanes whose items belong to the same neighbour are
+    // folded into acc[] by the lowest of them, in lane order, so every acc[]
+    // is a left-to-right sum in item order.
+    {
+        // the cavity-search scratch is free now: item buffer of one round
+        constexpr int PER = 4 * G;  // items of one round (old terms: 4 per lane)
+        static_assert(PER * (sizeof(double) + sizeof(int16_t)) <= sizeof(ws.u), "item buffer");
+        double *bterm = reinterpret_cast<double *>(&ws.u);
+        int16_t *bslot = reinterpret_cast<int16_t *>(bterm + PER);
+        // folds buffered items [0, n) into acc[]
+        auto fold = [&](int n) {
+            for (int k0 = 0; k0 < n; k0 += G) {
+                const int k = k0 + g.lane;
+                const int s = k < n ? bslot[k] : -1;
+                const double term = k < n ? bterm[k] : 0.0;
+                const unsigned peers = g.match(s);
+                const bool lead = s >= 0 && (__ffs(peers) - 1) == g.lane;
+                unsigned rem = lead ? peers : 0u;
+                double a = lead ? ws.acc[s] : 0.0;
+                while (g.any(rem != 0u)) {
+                    const int src = rem ? __ffs(rem) - 1 : g.lane;
+                    const double tv = g.shfl(term, src);
+                    if (rem) {
+                        a = fadd(a, tv);
+                        rem &= rem - 1u;
+                    }
+                }
+                if (lead) ws.acc[s] = a;
+                g.sync();
+            }
+        };
+        // cavity-tet terms (natural_insertionfree.c:642-676)
+        for (int o0 = 0; o0 < ncav; o0 += G) {
+            const int o = o0 + g.lane;
+            const int nt_round = min(G, ncav - o0);
+            if (o < ncav) {
+                const int c = ws.order[o];
                 const int tt = ws.cav_tet[c];
                 const int4 p = M.tv[tt];
-                const int v = comp(p, vi);
-                if (v < M.n) s = neighbour_slot(ws, v);
-                if (s >= 0) {
-                    const uint32_t info = M.tinfo[tt];
-                    // the other three vertices in ascending slot order
-                    const int o0 = (vi == 0) ? 1 : 0;
-                    const int o1 = (vi <= 1) ? 2 : 1;
-                    const int o2 = (vi <= 2) ? 3 : 2;
-                    pk = vload(M, v);
-                    pa = vload(M, comp(p, o0));
-                    pb = vload(M, comp(p, o1));
-                    pc = vload(M, comp(p, o2));
-                    ct = cload(&M.tcc[tt]);
-                    f1 = face_cc(M, ws, c, tt, info, o2);
-                    f2 = face_cc(M, ws, c, tt, info, o1);
-                    f3 = face_cc(M, ws, c, tt, info, o0);
+                const uint32_t info = M.tinfo[tt];
+                // circumcentres of the 4 faces as natinterp3d's face cache returns them
+                const d4 *fp[4];
+#pragma unroll
+                for (int i = 0; i < 4; i++) {
+                    const int j = 3 - i;
+                    const int nc = ws.cav_nbr[4 * c + j];
+                    if (nc >= 0 && ws.pos[nc] < ws.pos[c]) {
+                        const int jm = (info >> (8 + 2 * j)) & 3;
+                        fp[i] = &M.fcc[4 * (size_t)ws.cav_tet[nc] + (3 - jm)];
+                    } else {
+                        fp[i] = &M.fcc[4 * (size_t)tt + i];
+                    }
                 }
-            } else {
-                // virtual tet (query + boundary face), vertex j (:681-719)
-                const int kk = k - n_old;
-                const int b = kk / 3, j = kk - 3 * b;
+#pragma unroll 1
+                for (int vi = 0; vi < 4; vi++) {
+                    const int v = comp(p, vi);
+                    const int sl = v < M.n ? neighbour_slot(ws, v) : -1;
+                    double term = 0.0;
+                    if (sl >= 0) {
+                        // the other three vertices in ascending slot order
+                        const int o0v = (vi == 0) ? 1 : 0;
+                        const int o1v = (vi <= 1) ? 2 : 1;
+                        const int o2v = (vi <= 2) ? 3 : 2;
+                        const dv3 pk = vload(M, v);
+                        const dv3 pa = vload(M, comp(p, o0v));
+                        const dv3 pb = vload(M, comp(p, o1v));
+                        const dv3 pc = vload(M, comp(p, o2v));
+                        const dv3 ct = cload(&M.tcc[tt]);
+                        // fp[] indexed through selects, so that it stays in registers
+                        auto pick = [&](int i) {
+                            return i == 0 ? fp[0] : (i == 1 ? fp[1] : (i == 2 ? fp[2] : fp[3]));
+                        };
+                        const dv3 f1 = cload(pick(o2v));
+                        const dv3 f2 = cload(pick(o1v));
+                        const dv3 f3 = cload(pick(o0v));
+                        term = subcell_volume(pk, pa, pb, pc, ct, f1, f2, f3);
+                    }
+                    bterm[4 * g.lane + vi] = term;
+                    bslot[4 * g.lane + vi] = (int16_t)sl;
+                }
+            }
+            g.sync();
+            fold(4 * nt_round);
+        }
+        // virtual-tet terms, query + boundary face (:681-719)
+        for (int b0 = 0; b0 < nbf; b0 += G) {
+            const int b = b0 + g.lane;
+            const int nb_round = min(G, nbf - b0);
+            if (b < nbf) {
                 const int cf = ws.bface[b];
                 const int f = cf & 3;
                 const int tt = ws.cav_tet[cf >> 2];
@@ -761,39 +815,29 @@ __device__ RowInfo sibson_row(const MeshView &M, const dv3 q, W &ws, const Grp<G
                 const int va = comp(p, face_vslot(f, 0));
                 const int vb = comp(p, face_vslot(f, 1));
                 const int vc = comp(p, face_vslot(f, 2));
-                const int v = (j == 0) ? va : (j == 1 ? vb : vc);
-                if (v < M.n) s = neighbour_slot(ws, v);
-                if (s >= 0) {
-                    const dv3 fa = vload(M, va), fb = vload(M, vb), fc = vload(M, vc);
-                    pk = (j == 0) ? fa : (j == 1 ? fb : fc);
-                    pa = q;
-                    pb = (j == 0) ? fb : (j == 1 ? fc : fa);  // face_verts[(j+1)%3]
-                    pc = (j == 0) ? fc : (j == 1 ? fa : fb);  // face_verts[(j+2)%3]
-                    ct = tet_cc(q, fa, fb, fc);
-                    f1 = tri_cc(pk, q, pb);
-                    f2 = tri_cc(pk, q, pc);
-                    f3 = cload(&M.fcc[4 * (size_t)tt + (3 - f)]);
+                const dv3 fa = vload(M, va), fb = vload(M, vb), fc = vload(M, vc);
+                const dv3 f3 = cload(&M.fcc[4 * (size_t)tt + (3 - f)]);
+                const dv3 ct = tet_cc(q, fa, fb, fc);
+#pragma unroll 1
+                for (int j = 0; j < 3; j++) {
+                    const int v = (j == 0) ? va : (j == 1 ? vb : vc);
+                    const int sl = v < M.n ? neighbour_slot(ws, v) : -1;
+                    double term = 0.0;
+                    if (sl >= 0) {
+                        const dv3 pk = (j == 0) ? fa : (j == 1 ? fb : fc);
+                        const dv3 pb = (j == 0) ? fb : (j == 1 ? fc : fa);  // face_verts[(j+1)%3]
+                        const dv3 pc = (j == 0) ? fc : (j == 1 ? fa : fb);  // face_verts[(j+2)%3]
+                        const dv3 f1 = tri_cc(pk, q, pb);
+                        const dv3 f2 = tri_cc(pk, q, pc);
+                        term = -subcell_volume(pk, q, pb, pc, ct, f1, f2, f3);
+                    }
+                    bterm[3 * g.lane + j] = term;
+                    bslot[3 * g.lane + j] = (int16_t)sl;
                 }
             }
-            if (s >= 0) {
-                const double vol = subcell_volume(pk, pa, pb, pc, ct, f1, f2, f3);
-                term = old_term ? vol : -vol;
-            }
+            g.sync();
+            fold(3 * nb_round);
         }
-        const unsigned peers = g.match(s);
-        const bool lead = s >= 0 && (__ffs(peers) - 1) == g.lane;
-        unsigned rem = lead ? peers : 0u;
-        double a = lead ? ws.acc[s] : 0.0;
-        while (g.any(rem != 0u)) {
-            const int src = rem ? __ffs(rem) - 1 : g.lane;
-            const double tv = g.shfl(term, src);
-            if (rem) {
-                a = fadd(a, tv);
-                rem &= rem - 1u;
-            }
-        }
-        if (lead) ws.acc[s] = a;
-        g.sync();
     }
 
     // ---- 5. normalisation -----------------------------------------------------

@@ -81,6 +81,21 @@ class DeviceMesh:
                 'nif_dmesh_set_predicates')
         self.predicates = mode
 
+    def set_tuning(self, tuning):
+        """Launch settings of later query calls (``nif_tuning``: a dict with
+        ``blocks_per_sm`` 6 or 8, ``bucket_shift`` -2..1, ``tile`` 0..1024).
+        Results do not depend on them."""
+        t = N.Tuning.from_dict(tuning)
+        rc = self._lib.nif_dmesh_set_tuning(self._h, ctypes.byref(t))
+        if rc == N.NIF_ERR_ARG:
+            raise ValueError('invalid tuning %r' % (tuning,))
+        N.check(rc, 'nif_dmesh_set_tuning')
+
+    def get_tuning(self):
+        t = N.Tuning()
+        N.check(self._lib.nif_dmesh_get_tuning(self._h, ctypes.byref(t)), 'nif_dmesh_get_tuning')
+        return t.as_dict()
+
     @property
     def nbytes(self):
         return self._buf.numel()

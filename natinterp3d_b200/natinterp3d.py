@@ -146,7 +146,27 @@ class Interpolator:
         if self._dmesh is None:
             self._dmesh = DeviceMesh(*self.mesh_arrays, device=self._device_arg)
             self._dmesh.set_predicates(self._predicates)
+            if getattr(self, '_tuning', None) is not None:
+                self._dmesh.set_tuning(self._tuning)
         return self._dmesh
+
+    # ------------------------------------------------------------------ tuning
+    def set_tuning(self, tuning):
+        """Launch settings of the query kernels for the following calls
+        (``blocks_per_sm`` 6 or 8, ``bucket_shift`` -2..1, ``tile`` 0..1024);
+        they change speed only, never results."""
+        self.device_mesh.set_tuning(tuning)
+        self._tuning = dict(tuning)
+
+    @property
+    def tuning(self):
+        return self.device_mesh.get_tuning()
+
+    def tune(self, query_points, values=None, mode='interpolate', **kw):
+        """Time the candidate launch settings on (a sample of) these queries
+        and keep the fastest; see :func:`natinterp3d_b200.tuning.tune`."""
+        from .tuning import tune
+        return tune(self, query_points, values, mode=mode, **kw)
 
     def set_predicates(self, mode):
         """'fast', 'audit' or 'exact' for the following calls."""
