@@ -89,7 +89,7 @@ void *nif_mesh_native(const nif_mesh *h);
 typedef struct nif_dmesh nif_dmesh;
 
 /* Size in bytes of the device buffer that holds a resident mesh of
- * n_vertices (= keys + 4) and n_tets tets: vertices, tets, neighbours,
+ * n_vertices (= keys + 4) and n_tets (at most 2^29 - 1) tets: vertices, tets, neighbours,
  * orientation and mirror flags, cached tet and face circumcentres and the
  * point-location seed grid.  (natinterp3d keeps the mesh as pointer-linked
  * structs, delaunay.h:44-70, and re-packs it on first query,

@@ -1197,8 +1197,11 @@ int check_query_args(const nif_dmesh *m, const void *q, int qdt, int64_t M, cons
 // ---------------------------------------------------------------------------
 // exported API
 // ---------------------------------------------------------------------------
+// face-circumcentre indices 4 t + i must fit int32
+constexpr int MAX_TETS = INT_MAX / 4;
+
 NIF_EXPORT int nif_dmesh_bytes(int n_vertices, int n_tets, size_t *bytes) {
-    if (!bytes || n_vertices < 5 || n_tets < 1) return NIF_ERR_ARG;
+    if (!bytes || n_vertices < 5 || n_tets < 1 || n_tets > MAX_TETS) return NIF_ERR_ARG;
     Carve c{nullptr, 0, (size_t)-1, true};
     carve_mesh(c, n_vertices, n_tets);
     *bytes = align_up(c.off, 256);
@@ -1210,7 +1213,8 @@ NIF_EXPORT int nif_dmesh_create(const double *d_vxyz, const int32_t *d_tet_v,
                                 size_t buf_bytes, void *stream, nif_dmesh **out) {
     if (!out) return NIF_ERR_ARG;
     *out = nullptr;
-    if (!d_vxyz || !d_tet_v || !d_tet_n || !d_buf || n_vertices < 5 || n_tets < 1)
+    if (!d_vxyz || !d_tet_v || !d_tet_n || !d_buf || n_vertices < 5 || n_tets < 1 ||
+        n_tets > MAX_TETS)
         return NIF_ERR_ARG;
     if (reinterpret_cast<uintptr_t>(d_buf) % 256 != 0) return NIF_ERR_ARG;
     size_t need = 0;

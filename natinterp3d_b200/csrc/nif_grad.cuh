@@ -118,30 +118,30 @@ __device__ __forceinline__ dual3 subcell_volume_d(dvec pk, dvec pa, dvec pb, dve
 
 // Gradient of sum_j c_j * (virtual-tet term of vertex j) over the three
 // vertices of boundary face (fa, fb, fc); c_j = 0 skips a vertex.  The
-// virtual-tet circumcentre and the three (vertex, query, vertex) triangle
-// circumcentres are shared by the face's three terms (each triangle is
-// evaluated in one vertex order; its value part can differ from the other
-// order only in the last bits, which moves no branch of the volume formula).
+// virtual-tet circumcentre is shared by the face's three terms; each term
+// evaluates its two (vertex, query, vertex) triangle circumcentres in the
+// forward pass's own argument order (natural_insertionfree.c:708-714), so
+// its value part is bit-identical to the forward's.  One loop iteration per
+// term keeps the live dual state small (it would otherwise spill).
 __device__ __forceinline__ dv3 virtual_face_grad(dv3 q, dv3 fa, dv3 fb, dv3 fc, dv3 cface, double c0,
                                                  double c1, double c2) {
     const dvec Q = dvec{dual3{q.x, 1.0, 0.0, 0.0}, dual3{q.y, 0.0, 1.0, 0.0}, dual3{q.z, 0.0, 0.0, 1.0}};
-    const dvec A = dvconst(fa), B = dvconst(fb), C = dvconst(fc), F = dvconst(cface);
-    const dvec ct = tet_cc_d(Q, A, B, C);
-    const dvec tab = tri_cc_d(A, Q, B);
-    const dvec tac = tri_cc_d(A, Q, C);
-    const dvec tbc = tri_cc_d(B, Q, C);
+    const dvec ct = tet_cc_d(Q, dvconst(fa), dvconst(fb), dvconst(fc));
     dv3 gsum = dv3{0.0, 0.0, 0.0};
-    if (c0 != 0.0) {
-        const dual3 v = subcell_volume_d(A, Q, B, C, ct, tab, tac, F);
-        gsum.x += c0 * v.dx; gsum.y += c0 * v.dy; gsum.z += c0 * v.dz;
-    }
-    if (c1 != 0.0) {
-        const dual3 v = subcell_volume_d(B, Q, C, A, ct, tbc, tab, F);
-        gsum.x += c1 * v.dx; gsum.y += c1 * v.dy; gsum.z += c1 * v.dz;
-    }
-    if (c2 != 0.0) {
-        const dual3 v = subcell_volume_d(C, Q, A, B, ct, tac, tbc, F);
-        gsum.x += c2 * v.dx; gsum.y += c2 * v.dy; gsum.z += c2 * v.dz;
+#pragma unroll 1
+    for (int j = 0; j < 3; j++) {
+        const double cj = j == 0 ? c0 : (j == 1 ? c1 : c2);
+        if (cj == 0.0) continue;
+        const dv3 k = j == 0 ? fa : (j == 1 ? fb : fc);
+        const dv3 n = j == 0 ? fb : (j == 1 ? fc : fa);  // face_verts[(j+1)%3]
+        const dv3 p = j == 0 ? fc : (j == 1 ? fa : fb);  // face_verts[(j+2)%3]
+        const dvec K = dvconst(k), N = dvconst(n), P = dvconst(p);
+        const dvec t1 = tri_cc_d(K, Q, N);
+        const dvec t2 = tri_cc_d(K, Q, P);
+        const dual3 v = subcell_volume_d(K, Q, N, P, ct, t1, t2, dvconst(cface));
+        gsum.x += cj * v.dx;
+        gsum.y += cj * v.dy;
+        gsum.z += cj * v.dz;
     }
     return gsum;
 }

@@ -759,17 +759,18 @@ __device__ RowInfo sibson_row(const MeshView &M, const dv3 q, W &ws, const Grp<G
                 const int tt = ws.cav_tet[c];
                 const int4 p = M.tv[tt];
                 const uint32_t info = M.tinfo[tt];
-                // circumcentres of the 4 faces as natinterp3d's face cache returns them
-                const d4 *fp[4];
+                // circumcentres of the 4 faces as natinterp3d's face cache returns
+                // them, as fcc[] indices (4 T < 2^31: nif_dmesh_create limits T)
+                int fp[4];
 #pragma unroll
                 for (int i = 0; i < 4; i++) {
                     const int j = 3 - i;
                     const int nc = ws.cav_nbr[4 * c + j];
                     if (nc >= 0 && ws.pos[nc] < ws.pos[c]) {
                         const int jm = (info >> (8 + 2 * j)) & 3;
-                        fp[i] = &M.fcc[4 * (size_t)ws.cav_tet[nc] + (3 - jm)];
+                        fp[i] = 4 * ws.cav_tet[nc] + (3 - jm);
                     } else {
-                        fp[i] = &M.fcc[4 * (size_t)tt + i];
+                        fp[i] = 4 * tt + i;
                     }
                 }
 #pragma unroll 1
@@ -791,9 +792,9 @@ __device__ RowInfo sibson_row(const MeshView &M, const dv3 q, W &ws, const Grp<G
                         auto pick = [&](int i) {
                             return i == 0 ? fp[0] : (i == 1 ? fp[1] : (i == 2 ? fp[2] : fp[3]));
                         };
-                        const dv3 f1 = cload(pick(o2v));
-                        const dv3 f2 = cload(pick(o1v));
-                        const dv3 f3 = cload(pick(o0v));
+                        const dv3 f1 = cload(&M.fcc[pick(o2v)]);
+                        const dv3 f2 = cload(&M.fcc[pick(o1v)]);
+                        const dv3 f3 = cload(&M.fcc[pick(o0v)]);
                         term = subcell_volume(pk, pa, pb, pc, ct, f1, f2, f3);
                     }
                     bterm[4 * g.lane + vi] = term;
@@ -815,21 +816,22 @@ __device__ RowInfo sibson_row(const MeshView &M, const dv3 q, W &ws, const Grp<G
                 const int va = comp(p, face_vslot(f, 0));
                 const int vb = comp(p, face_vslot(f, 1));
                 const int vc = comp(p, face_vslot(f, 2));
-                const dv3 fa = vload(M, va), fb = vload(M, vb), fc = vload(M, vc);
-                const dv3 f3 = cload(&M.fcc[4 * (size_t)tt + (3 - f)]);
-                const dv3 ct = tet_cc(q, fa, fb, fc);
+                const dv3 ct = tet_cc(q, vload(M, va), vload(M, vb), vload(M, vc));
+                const int ffi = 4 * tt + (3 - f);
 #pragma unroll 1
                 for (int j = 0; j < 3; j++) {
                     const int v = (j == 0) ? va : (j == 1 ? vb : vc);
                     const int sl = v < M.n ? neighbour_slot(ws, v) : -1;
                     double term = 0.0;
                     if (sl >= 0) {
-                        const dv3 pk = (j == 0) ? fa : (j == 1 ? fb : fc);
-                        const dv3 pb = (j == 0) ? fb : (j == 1 ? fc : fa);  // face_verts[(j+1)%3]
-                        const dv3 pc = (j == 0) ? fc : (j == 1 ? fa : fb);  // face_verts[(j+2)%3]
+                        // the face's vertices are re-read (L1) rather than held
+                        // across the loop, which would spill them
+                        const int vn = (j == 0) ? vb : (j == 1 ? vc : va);  // face_verts[(j+1)%3]
+                        const int vp = (j == 0) ? vc : (j == 1 ? va : vb);  // face_verts[(j+2)%3]
+                        const dv3 pk = vload(M, v), pb = vload(M, vn), pc = vload(M, vp);
                         const dv3 f1 = tri_cc(pk, q, pb);
                         const dv3 f2 = tri_cc(pk, q, pc);
-                        term = -subcell_volume(pk, q, pb, pc, ct, f1, f2, f3);
+                        term = -subcell_volume(pk, q, pb, pc, ct, f1, f2, cload(&M.fcc[ffi]));
                     }
                     bterm[3 * g.lane + j] = term;
                     bslot[3 * g.lane + j] = (int16_t)sl;
