@@ -546,11 +546,11 @@ def main():
                 'phase_ms': {'bucketing': float(np.mean(kms[:, 0])), 'rows_fast': rows_ms,
                              'rows_large': float(np.mean(kms[:, 2])),
                              'epilogue': float(np.mean(kms[:, 3]))},
-                # dram__bytes_read.sum + dram__bytes_write.sum of one k_rows_fast launch at
-                # 200k keys / 2M queries (profiles/k_rows_fast_200k_keys_2M_queries.md),
-                # scaled by this launch's queries (the mesh scales with the keys alike)
-                'traffic': 802.0e6 * (M / 2_000_000),
-                'traffic_note': 'ncu capture at 200k keys / 2M queries scaled by queries',
+                # dram__bytes_read.sum + dram__bytes_write.sum of one full-size k_rows_fast
+                # launch (1M keys, 10M queries, tuning 8,0,8; profiles/launches_1M_keys_10M_queries.md),
+                # scaled by this launch's query count
+                'traffic': 4.4257e9 * (M / 10_000_000),
+                'traffic_note': 'ncu capture of one k_rows_fast launch at 1M keys / 10M queries',
             },
             'cpu_baseline': cpu,
             'e2e': {'value': M * world / e2e_sec, 'unit': 'queries/s',
