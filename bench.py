@@ -362,6 +362,16 @@ def run_batched(args, rank, world, local_rank):
 
     ms_graph = timed(graph.replay)
     ms_loop = timed(lambda: b.interpolate_per_problem(qcat, qoff, vcat))
+    # the same loop through the default device API: each call checks its rows
+    # (reads the row counters back, so it synchronises once per problem)
+    qo, ko = qoff, b.key_offsets.cpu().numpy()
+
+    def api_loop():
+        for p, it in enumerate(b.interpolators):
+            if qo[p + 1] > qo[p]:
+                it.interpolate_device(qcat[qo[p]:qo[p + 1]], vcat[ko[p]:ko[p + 1]])
+
+    ms_api = timed(api_loop)
     # host API: one Interpolator.interpolate per problem (numpy in and out) vs one batched call
     t0 = time.perf_counter()
     for p in range(args.problems):
@@ -389,6 +399,7 @@ def run_batched(args, rank, world, local_rank):
             'metric': METRIC, 'mode': 'batched', 'value': M / (ms_graph * 1e-3), 'unit': 'queries/s',
             'n_gpus': world, 'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': ms_graph,
             'per_problem_launches_ms': ms_loop, 'batched_over_per_problem_speedup': ms_loop / ms_graph,
+            'per_problem_api_ms': ms_api, 'batched_over_per_problem_api': ms_api / ms_graph,
             'host_api_per_problem_s': host_loop_s, 'host_api_batched_s': host_batch_s,
             'host_api_speedup': host_loop_s / host_batch_s,
             'bit_identical_to_per_problem': same, 'higher_is_better': True, 'dtype': 'f64',
@@ -456,11 +467,17 @@ def main():
     # autotuner (setup, untimed): launch settings for this workload, timed on
     # a 2M-query sample; results do not depend on them
     t0 = time.perf_counter()
-    tuned = None
+    tuned = tune_times = None
     if fixed_tuning(args):
         interp.set_tuning(fixed_tuning(args))
     elif not args.no_tune:
-        tuned = interp.tune(qd, vd, use_cache=False)['tuning']
+        rep = interp.tune(qd, vd, use_cache=False)
+        tuned = rep['tuning']
+        # the 2M-query sample's time of the library default and of the pick
+        times = {tuple(sorted(c.items())): t for c, t in rep['times_ms']}
+        dflt = {'blocks_per_sm': 8, 'bucket_shift': 0, 'tile': 8}
+        tune_times = {'default_ms': times.get(tuple(sorted(dflt.items()))),
+                      'chosen_ms': times.get(tuple(sorted(tuned.items())))}
     tune_s = time.perf_counter() - t0
 
     def step():
@@ -533,7 +550,7 @@ def main():
                 'tets': dm.n_tets, 'bit_identical_to_oracle_on_sample': exact,
                 'predicates': args.predicates,
                 'tuning': dm.get_tuning(), 'autotuned': tuned is not None,
-                'tune_s': round(tune_s, 2),
+                'tune_s': round(tune_s, 2), 'tune_sample_ms': tune_times,
             },
             'roofline': {
                 'bound': 'fp64', 'kernel': 'k_rows_fast',

@@ -145,12 +145,16 @@ int nif_dmesh_set_predicates(nif_dmesh *m, int mode);
  *   tile           queries a warp takes per work item: 0 = a static grid
  *                  stride (one query per step), 1 .. 1024 = tiles of
  *                  consecutive bucket-ordered queries pulled from a device
- *                  counter
+ *                  counter.  For one mesh this is an upper bound: a call with
+ *                  fewer than 2 x tile queries per resident warp uses smaller
+ *                  tiles, or the static stride, so small calls fill the GPU
  * nif_dmesh_set_tuning applies to later query calls on the mesh (the
  * workspace size depends on bucket_shift: query nif_query_workspace_bytes
  * after setting it); nif_batch_set_tuning to later batch calls, which ignore
- * bucket_shift and need tile >= 1.  nif_interpolate_noalloc uses only
- * blocks_per_sm.  Defaults: {8, 0, 0} for a mesh, {8, 0, 64} for a batch.
+ * bucket_shift and need tile >= 1.  nif_interpolate_noalloc follows the
+ * mesh's settings with bucket_shift capped at 0 (its fixed scratch holds the
+ * default bucket count).  Defaults: {8, 0, 8} for a mesh, {8, 0, 64} for a
+ * batch.
  * Out-of-range values return NIF_ERR_ARG and change nothing. */
 typedef struct {
     int32_t blocks_per_sm;

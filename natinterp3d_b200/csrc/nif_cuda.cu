@@ -46,6 +46,7 @@ constexpr int OCC_LO = 6;   // 80 registers a thread
 constexpr int OCC_HI = 8;   // 64 registers a thread
 constexpr int OCC_DEFAULT = OCC_HI;
 constexpr int TILE_MAX = 1024;
+constexpr int MESH_TILE_DEFAULT = 8;   // queries per work item of a single mesh's row kernel
 constexpr int BATCH_TILE_DEFAULT = 64;
 constexpr int FAST_G = NIF_FAST_G;    // lanes per query in the shared-memory kernel
 using FastWS = Workspace<256, 96, 128, 64, 128, FAST_G, uint8_t, int8_t>;
@@ -916,7 +917,7 @@ struct nif_dmesh {
     int num_sms;
     size_t bytes;
     int64_t orient_unc, orient_flip;  // tets with an uncertain / flipped orientation flag
-    nif_tuning tune{OCC_DEFAULT, 0, 0, 0};
+    nif_tuning tune{OCC_DEFAULT, 0, MESH_TILE_DEFAULT, 0};
 };
 
 namespace {
@@ -1111,7 +1112,14 @@ void launch_fast_occ(const nif_dmesh *m, const QT *Q, int64_t M, const Centroid 
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, FAST_BLOCK, smem);
         if (per_sm < 1) per_sm = 1;
     }
-    const int tile = m->tune.tile;
+    // tile is an upper bound: a call too small to give every resident group
+    // two tiles takes smaller ones (or the static stride), so that small
+    // calls keep the whole GPU busy
+    int tile = m->tune.tile;
+    if (tile > 0) {
+        const int64_t fit = M / (2 * (int64_t)per_sm * m->num_sms * GPB);
+        if (fit < tile) tile = (int)fit;
+    }
     int64_t blocks = (M + GPB - 1) / GPB;
     if (tile > 0) blocks = (M + (int64_t)GPB * tile - 1) / ((int64_t)GPB * tile);
     const int64_t cap = (int64_t)per_sm * m->num_sms;

@@ -42,7 +42,7 @@ import torch
 __all__ = ['MESH_CANDIDATES', 'BATCH_CANDIDATES', 'tune', 'tune_batch', 'cache_path']
 
 MESH_CANDIDATES = [{'blocks_per_sm': b, 'tile': t, 'bucket_shift': s}
-                   for b, t, s in itertools.product((8, 6), (0, 8, 32), (0, -1, 1))]
+                   for b, t, s in itertools.product((8, 6), (8, 0, 32), (0, -1, 1))]
 BATCH_CANDIDATES = [{'blocks_per_sm': b, 'tile': t, 'bucket_shift': 0}
                     for b, t in itertools.product((8, 6), (64, 16, 32, 128))]
 

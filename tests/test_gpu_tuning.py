@@ -31,7 +31,7 @@ def case(cuda_device):
 
 def test_default_tuning(case):
     I, _, _ = case
-    assert I.tuning == {'blocks_per_sm': 8, 'bucket_shift': 0, 'tile': 0}
+    assert I.tuning == {'blocks_per_sm': 8, 'bucket_shift': 0, 'tile': 8}
 
 
 @pytest.mark.parametrize('cand', tuning.MESH_CANDIDATES + [
@@ -39,14 +39,14 @@ def test_default_tuning(case):
     {'blocks_per_sm': 8, 'tile': 1024, 'bucket_shift': 1}])
 def test_every_setting_gives_identical_results(case, cand):
     I, qd, vd = case
-    I.set_tuning({'blocks_per_sm': 8, 'bucket_shift': 0, 'tile': 0})
+    I.set_tuning({'blocks_per_sm': 8, 'bucket_shift': 0, 'tile': 8})
     ref_out = I.interpolate_device(qd, vd)
     ref_w = I.get_weights_device(qd)
     I.set_tuning(cand)
     assert I.tuning == cand
     out = I.interpolate_device(qd, vd)
     w = I.get_weights_device(qd)
-    I.set_tuning({'blocks_per_sm': 8, 'bucket_shift': 0, 'tile': 0})
+    I.set_tuning({'blocks_per_sm': 8, 'bucket_shift': 0, 'tile': 8})
     assert torch.equal(out, ref_out)
     for a, b in zip(w, ref_w):
         assert torch.equal(a, b)
@@ -73,7 +73,7 @@ def test_workspace_size_does_not_depend_on_tuning(case):
     for s in (-2, 0, 1):
         I.set_tuning({'blocks_per_sm': 8, 'tile': 0, 'bucket_shift': s})
         sizes.add(dm.workspace_bytes(qd.shape[0], N.NIF_MODE_WEIGHTS))
-    I.set_tuning({'blocks_per_sm': 8, 'bucket_shift': 0, 'tile': 0})
+    I.set_tuning({'blocks_per_sm': 8, 'bucket_shift': 0, 'tile': 8})
     assert len(sizes) == 1
 
 
@@ -96,7 +96,7 @@ def test_noalloc_follows_tuning_with_capped_buckets(case):
                 'nif_interpolate_noalloc')
         assert summ.rows_failed == 0
         assert torch.equal(out, ref)
-    I.set_tuning({'blocks_per_sm': 8, 'bucket_shift': 0, 'tile': 0})
+    I.set_tuning({'blocks_per_sm': 8, 'bucket_shift': 0, 'tile': 8})
 
 
 def test_autotuner_keeps_a_candidate_and_caches_it(case, tmp_path, monkeypatch):
@@ -113,7 +113,7 @@ def test_autotuner_keeps_a_candidate_and_caches_it(case, tmp_path, monkeypatch):
     assert rep2['cached'] and rep2['tuning'] == rep['tuning'] and I.tuning == rep['tuning']
     rep3 = I.tune(qd, mode='weights', reps=1, candidates=tuning.MESH_CANDIDATES[:3])
     assert rep3['tuning'] in tuning.MESH_CANDIDATES[:3]
-    I.set_tuning({'blocks_per_sm': 8, 'bucket_shift': 0, 'tile': 0})
+    I.set_tuning({'blocks_per_sm': 8, 'bucket_shift': 0, 'tile': 8})
 
 
 def test_batch_settings_and_tuner(cuda_device, tmp_path, monkeypatch):
