@@ -349,21 +349,6 @@ __device__ int canonical_start(const MeshView &M, const W &ws, const Grp<G> &g, 
     return best_c;
 }
 
-// Circumcentre natinterp3d's face cache returns for the face opposite p[i] of
-// cavity tet c (tet id t, tinfo word info): the value cached by whichever of
-// the two cavity tets sharing the face natinterp3d visits first.
-template <class W>
-__device__ __forceinline__ dv3 face_cc(const MeshView &M, const W &ws, int c, int t, uint32_t info,
-                                      int i) {
-    const int j = 3 - i;
-    const int nc = ws.cav_nbr[4 * c + j];
-    if (nc >= 0 && ws.pos[nc] < ws.pos[c]) {
-        const int jm = (info >> (8 + 2 * j)) & 3;
-        return cload(&M.fcc[4 * (size_t)ws.cav_tet[nc] + (3 - jm)]);
-    }
-    return cload(&M.fcc[4 * (size_t)t + i]);
-}
-
 // slot of a data vertex among the natural neighbours, -1 if it is not one
 template <class W>
 __device__ __forceinline__ int neighbour_slot(const W &ws, int v) {
@@ -760,7 +745,10 @@ __device__ RowInfo sibson_row(const MeshView &M, const dv3 q, W &ws, const Grp<G
                 const int4 p = M.tv[tt];
                 const uint32_t info = M.tinfo[tt];
                 // circumcentres of the 4 faces as natinterp3d's face cache returns
-                // them, as fcc[] indices (4 T < 2^31: nif_dmesh_create limits T)
+                // them (natural_insertionfree.c:233-253): for a face shared with
+                // another cavity tet, the copy cached by whichever of the two
+                // natinterp3d visits first (its mirror slot is in tinfo); as
+                // fcc[] indices (4 T < 2^31: nif_dmesh_create limits T)
                 int fp[4];
 #pragma unroll
                 for (int i = 0; i < 4; i++) {
