@@ -19,6 +19,7 @@ import torch
 
 from . import _native as N
 from .device import _DT, DeviceMesh, _stream_ptr, _vp
+from . import natinterp3d as _api
 from .natinterp3d import Interpolator
 
 __all__ = ['BatchInterpolator', 'BatchGraph']
@@ -141,14 +142,93 @@ class BatchInterpolator:
             raise ValueError('need one query array and one value array per problem')
         vals = [np.asarray(v) for v in values_list]
         squeeze = vals[0].ndim == 1
-        qcat = np.concatenate([np.asarray(q, np.float64).reshape(-1, 3) for q in queries_list])
-        vcat = np.concatenate([v.reshape(v.shape[0], -1) for v in vals])
-        qoff = self.query_offsets([len(q) for q in queries_list])
-        out = self.interpolate_device(torch.from_numpy(qcat).to(self.device), qoff,
-                                      torch.from_numpy(np.ascontiguousarray(vcat)).to(self.device))
-        out = out.cpu().numpy()
+        qs = [np.asarray(q, np.float64).reshape(-1, 3) for q in queries_list]
+        qoff = self.query_offsets([len(q) for q in qs])
+        if qoff[-1] > 2 * _api.PIPELINE_CHUNK:
+            out = self._interpolate_pipelined(qs, qoff, vals)
+        else:
+            qcat = np.concatenate(qs)
+            vcat = np.concatenate([v.reshape(v.shape[0], -1) for v in vals])
+            out = self.interpolate_device(torch.from_numpy(qcat).to(self.device), qoff,
+                                          torch.from_numpy(np.ascontiguousarray(vcat)).to(self.device))
+            out = out.cpu().numpy()
         parts = [out[qoff[p]:qoff[p + 1]] for p in range(self.P)]
         return [p[:, 0] for p in parts] if squeeze else parts
+
+    def _interpolate_pipelined(self, qs, qoff, vals):
+        """Large host batches in groups of consecutive problems (about
+        PIPELINE_CHUNK queries each): while one group's batch call runs, the
+        next group's queries and values go to the device and the previous
+        group's results come back, on a separate copy stream through pinned
+        staging buffers.  Each call sees the other problems as empty (zero
+        queries), so its results are those of the whole batch.  Row counters
+        are read once at the end."""
+        dev = self.device
+        M = int(qoff[-1])
+        D = int(vals[0].reshape(vals[0].shape[0], -1).shape[1])
+        vdt = torch.float32 if all(v.dtype == np.float32 for v in vals) else torch.float64
+        odt = torch.float64  # queries are float64 on this path
+        out = np.empty((M, D), np.float64)
+        ko = self.key_offsets.cpu().numpy()
+        groups, p0 = [], 0
+        while p0 < self.P:
+            p1 = p0 + 1
+            while p1 < self.P and qoff[p1 + 1] - qoff[p0] <= _api.PIPELINE_CHUNK:
+                p1 += 1
+            groups.append((p0, p1))
+            p0 = p1
+        cap = max(int(qoff[b] - qoff[a]) for a, b in groups)
+        kcap = max(int(ko[b] - ko[a]) for a, b in groups)
+        compute = torch.cuda.current_stream(dev)
+        copy = torch.cuda.Stream(device=dev)
+        qstage = [torch.empty((cap, 3), dtype=torch.float64, pin_memory=True) for _ in range(2)]
+        vstage = [torch.empty((kcap, D), dtype=vdt, pin_memory=True) for _ in range(2)]
+        ostage = [torch.empty((cap, D), dtype=odt, pin_memory=True) for _ in range(2)]
+        with torch.cuda.device(dev):
+            vd = torch.empty((int(ko[-1]), D), dtype=vdt, device=dev)
+            pending, checks = None, []
+
+            def drain(item):
+                slot, (a, b), res, done = item
+                copy.wait_event(done)
+                with torch.cuda.stream(copy):
+                    ostage[slot][:b - a].copy_(res, non_blocking=True)
+                    res.record_stream(copy)
+                copy.synchronize()
+                out[a:b] = ostage[slot][:b - a].numpy()
+
+            for k, (g0, g1) in enumerate(groups):
+                a, b = int(qoff[g0]), int(qoff[g1])
+                ka, kb = int(ko[g0]), int(ko[g1])
+                slot = k % 2
+                qn, vn = qstage[slot].numpy(), vstage[slot].numpy()
+                np.concatenate(qs[g0:g1], out=qn[:b - a])
+                np.concatenate([v.reshape(v.shape[0], -1) for v in vals[g0:g1]], out=vn[:kb - ka],
+                               casting='same_kind')
+                goff = torch.from_numpy(np.clip(qoff - a, 0, b - a))
+                with torch.cuda.stream(copy):
+                    qd = qstage[slot][:b - a].to(dev, non_blocking=True)
+                    vd[ka:kb].copy_(vstage[slot][:kb - ka], non_blocking=True)
+                    gd = goff.to(dev, non_blocking=True)
+                    loaded = torch.cuda.Event()
+                    loaded.record(copy)
+                compute.wait_event(loaded)
+                qd.record_stream(compute)
+                gd.record_stream(compute)
+                res = torch.empty((b - a, D), dtype=odt, device=dev)
+                ws = self.workspace(b - a)
+                self._launch(qd, gd, vd, res, ws)
+                checks.append((b - a, ws))
+                done = torch.cuda.Event()
+                done.record(compute)
+                if pending is not None:
+                    drain(pending)
+                    # the staging slot of the drained group is free again
+                pending = (slot, (a, b), res, done)
+            drain(pending)
+            for n, ws in checks:
+                DeviceMesh._raise_rows(self.summary(n, ws))
+        return out
 
     def interpolate_per_problem(self, queries, query_offsets, values):
         """The same result with one plain call per problem (for comparison)."""

@@ -71,3 +71,23 @@ def test_batch_float64_scalar_values(cuda_device):
     for p in range(5):
         assert outs[p].shape == (len(queries[p]),)
         assert np.array_equal(outs[p], b.interpolators[p].interpolate(queries[p], values[p]))
+
+
+@pytest.mark.parametrize('chunk', [1000, 4000])
+def test_pipelined_host_batch_matches_single_call(batch_case, monkeypatch, chunk):
+    """Host batches above two pipeline chunks go through problem groups on a
+    copy stream; the results equal the single-call path bit for bit."""
+    import natinterp3d_b200.natinterp3d as api
+    b, keys, queries, values, qoff, qcat, vcat = batch_case
+    ref = b.interpolate(queries, values)
+    monkeypatch.setattr(api, 'PIPELINE_CHUNK', chunk)
+    assert qoff[-1] > 2 * chunk
+    outs = b.interpolate(queries, values)
+    for p in range(b.P):
+        assert outs[p].dtype == ref[p].dtype and np.array_equal(outs[p], ref[p])
+    scal = [v[:, 0].astype(np.float64) for v in values]
+    outs = b.interpolate(queries, scal)
+    monkeypatch.setattr(api, 'PIPELINE_CHUNK', 1 << 21)
+    ref = b.interpolate(queries, scal)
+    for p in range(b.P):
+        assert outs[p].shape == (len(queries[p]),) and np.array_equal(outs[p], ref[p])
