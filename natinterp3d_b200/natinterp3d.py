@@ -37,6 +37,24 @@ _FLOATS = (np.dtype(np.float32), np.dtype(np.float64))
 PIPELINE_CHUNK = 1 << 21  # queries per chunk of the pipelined host interpolation
 
 
+def pipeline_bounds(M, chunk):
+    """Row ranges of a pipelined call: full chunks, with a first and a last
+    chunk of chunk/8 rows, whose upload and whose download plus host copy are
+    the only transfers that cannot overlap a kernel."""
+    small = max(1, chunk // 8)
+    first = min(M, small)
+    bounds, a = [(0, first)], first
+    while M - a > chunk + small:
+        bounds.append((a, a + chunk))
+        a += chunk
+    if M - a > small:
+        bounds.append((a, M - small))
+        a = M - small
+    if M > a:
+        bounds.append((a, M))
+    return bounds
+
+
 def interpolate(
     queries: np.ndarray,
     keys: np.ndarray,
@@ -250,7 +268,7 @@ class Interpolator:
         D = 1 if vd.dim() == 1 else int(vd.shape[1])
         odt = torch.float32 if (q.dtype == np.float32 and vd.dtype == torch.float32) else torch.float64
         out = np.empty((M, D), dtype=np.float32 if odt == torch.float32 else np.float64)
-        bounds = [(a, min(M, a + PIPELINE_CHUNK)) for a in range(0, M, PIPELINE_CHUNK)]
+        bounds = pipeline_bounds(M, PIPELINE_CHUNK)
         compute = torch.cuda.current_stream(dev)
         copy = torch.cuda.Stream(device=dev)
         staging = [torch.empty((PIPELINE_CHUNK, D), dtype=odt, pin_memory=True) for _ in range(2)]
