@@ -8,8 +8,11 @@
 //                                 nearby tets and the mesh stays in L1/L2;
 //                                 natinterp3d sorts by Morton code for the
 //                                 same reason (natural.c:70-96)
-//   k_rows<fast>                  one group of G lanes per query, scratch in
-//                                 shared memory; rows that exceed its
+//   k_rows<fast>                  one warp (G = 32 lanes) per query, scratch
+//                                 in shared memory, a persistent grid of 6 or
+//                                 8 blocks per SM taking rows by static
+//                                 stride or in tiles from a device counter
+//                                 (nif_tuning); rows that exceed its
 //                                 per-query capacities are queued
 //   k_rows<large>                 the queued rows, one warp each, scratch in a
 //                                 global-memory workspace with much larger
