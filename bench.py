@@ -250,6 +250,33 @@ def cpu_baseline(interp, queries, values):
                           sample, nthreads, sec)}
 
 
+def fwdbwd_cpu_baseline(interp, queries, values, gout):
+    """natinterp3d's own code for the differentiable step's CPU equivalent: its
+    weights (all host threads, same mesh object), scipy W @ values and the
+    values gradient W.T @ gout.  natinterp3d has no query gradient, so that
+    term has no CPU counterpart."""
+    from oracle import oracle
+    if not oracle.ref_available() or interp.host_mesh is None:
+        return None
+    nthreads = host_threads()
+    ptr = interp.host_mesh.native_pointer()
+    c = interp.centroid
+
+    def run(qs, gs):
+        W = oracle.ref_query(ptr, np.ascontiguousarray(qs, np.float64) - c, interp.n_keys, nthreads)
+        return W @ values, W.T @ gs
+
+    n = min(queries.shape[0], 100_000)
+    run(queries[:n // 10], gout[:n // 10])
+    t0 = time.perf_counter()
+    run(queries[:n], gout[:n])
+    sec = time.perf_counter() - t0
+    return {'value': n / sec, 'unit': 'queries/s', 'cores': nthreads, 'kind': 'reference',
+            'sample': '%d queries of the workload: natinterp3d getInsertionFreeWeightsParallel '
+                      '(%d threads) on the same mesh + scipy W @ values + W.T @ gout, %.2f s'
+                      % (n, nthreads, sec)}
+
+
 def run_fwdbwd(args, rank, world, local_rank):
     """Differentiable workload: loss = sum(out * g), backward into queries and values."""
     import torch
@@ -262,10 +289,12 @@ def run_fwdbwd(args, rank, world, local_rank):
     dev = torch.device('cuda', local_rank)
     rng = np.random.default_rng([3, rank])
     keys = rng.uniform(0, 1, (keys_n, 3))
-    interp = ni.Interpolator(keys, device=dev)
-    qd = torch.from_numpy(rng.uniform(0.1, 0.9, (q_n, 3))).to(dev)
-    vd = torch.from_numpy(rng.standard_normal((keys_n, dim)).astype(np.float32)).to(dev)
-    gd = torch.from_numpy(rng.standard_normal((q_n, dim))).to(dev)
+    interp = ni.Interpolator(keys, device=dev,
+                             keep_host_mesh=(rank == 0 and not args.no_cpu_baseline))
+    qn = rng.uniform(0.1, 0.9, (q_n, 3))
+    vn = rng.standard_normal((keys_n, dim)).astype(np.float32)
+    gn = rng.standard_normal((q_n, dim))
+    qd, vd, gd = (torch.from_numpy(a).to(dev) for a in (qn, vn, gn))
     # autotuner (setup, untimed) on the weights path the differentiable forward uses
     tuned = None
     if fixed_tuning(args):
@@ -297,11 +326,13 @@ def run_fwdbwd(args, rank, world, local_rank):
 
     ms_fwd = timed(fwd)
     ms_fb = timed(fwdbwd)
+    cpu = None if (args.no_cpu_baseline or rank != 0) else fwdbwd_cpu_baseline(interp, qn, vn, gn)
     if rank == 0:
         print(json.dumps({
             'metric': METRIC, 'mode': 'fwd+bwd', 'value': q_n / (ms_fb * 1e-3), 'unit': 'queries/s',
             'n_gpus': world, 'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': ms_fb,
             'plain_forward_ms': ms_fwd, 'fwdbwd_over_forward': ms_fb / ms_fwd,
+            'cpu_baseline': cpu,
             'higher_is_better': True, 'dtype': 'f64', 'data': 'synthetic',
             'config': {'workload': 'differentiable: %d keys U[0,1]^3, %d queries U[0.1,0.9]^3 float64 '
                                    'with grad, values D=%d float32 with grad, loss=sum(out*g), seed 3'
