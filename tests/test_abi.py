@@ -76,3 +76,31 @@ def test_degenerate_keys_rejected():
         HostMesh(flat)
     with pytest.raises(ValueError):
         HostMesh(np.zeros((5, 2)))
+
+
+def test_ctypes_mirrors_match_the_header_layout(tmp_path):
+    """nif_summary and nif_tuning as the C compiler lays them out from the
+    header, against the ctypes structures the package passes to the library."""
+    import shutil
+    import subprocess
+    from natinterp3d_b200 import _native
+    cc = shutil.which('gcc') or shutil.which('cc')
+    if cc is None:
+        pytest.skip('no C compiler')
+    src = tmp_path / 'layout.c'
+    src.write_text(
+        '#include <stdio.h>\n#include <stddef.h>\n#include "natinterp3d_b200.h"\n'
+        'int main(void) {\n'
+        '  printf("%zu %zu %zu %zu\\n", sizeof(nif_summary), offsetof(nif_summary, first_status),\n'
+        '         offsetof(nif_summary, orient_uncertain), offsetof(nif_summary, insphere_flipped));\n'
+        '  printf("%zu %zu %zu\\n", sizeof(nif_tuning), offsetof(nif_tuning, bucket_shift),\n'
+        '         offsetof(nif_tuning, tile));\n'
+        '  return 0;\n}\n')
+    exe = tmp_path / 'layout'
+    subprocess.run([cc, '-I', os.path.join(ROOT, 'include'), str(src), '-o', str(exe)], check=True)
+    lines = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split('\n')
+    S, T = _native.Summary, _native.Tuning
+    assert [int(x) for x in lines[0].split()] == [
+        ctypes.sizeof(S), S.first_status.offset, S.orient_uncertain.offset, S.insphere_flipped.offset]
+    assert [int(x) for x in lines[1].split()] == [
+        ctypes.sizeof(T), T.bucket_shift.offset, T.tile.offset]
