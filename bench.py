@@ -37,6 +37,11 @@ METRIC = 'Sibson queries/s at 1M keys (plain, fwd+bwd, batched) vs CPU OpenMP, 1
 WORKLOAD = ('plain interpolate at scale: {keys:,} keys U[0,1]^3 float64, {queries:,} queries '
             'U[0.02,0.98]^3 float64, values D={dim} float32 N(0,1), seed {seed}')
 
+# DRAM bytes (read + write) per query of one k_rows_fast launch, from an ncu
+# capture of the plain workload (profiles/launches_1M_keys_10M_queries.md)
+TRAFFIC_PER_QUERY = 4.4257e9 / 10_000_000
+TRAFFIC_SOURCE = '1M keys / 10M queries, profiles/launches_1M_keys_10M_queries.md'
+
 # FP64 operations per unit of work, counted as natinterp3d's C evaluates them
 # (each add, subtract, multiply and divide is one flop; no fused multiply-add)
 FLOPS = {'orient': 23, 'insphere': 77, 'tet_cc': 79, 'tri_cc': 56, 'subcell': 89}
@@ -63,6 +68,8 @@ def parse():
                         'batched: 512 uneven problems (keys log-uniform [500, 100k], queries '
                         'log-uniform [1k, 200k], boxes of side 0.5-2, D=4 float32, seed 4)')
     p.add_argument('--problems', type=int, default=512)
+    p.add_argument('--no-legs', action='store_true',
+                   help='plain leg only (skip get_weights, fwd+bwd and batched sub-results)')
     p.add_argument('--no-tune', action='store_true',
                    help="skip the autotuner (untimed setup) and keep the library's default "
                         "launch settings")
@@ -172,8 +179,22 @@ def flops_per_query(stats, gpu_walk_steps, n):
     return total / q
 
 
+def plain_config(args, world):
+    """The workload keys both arms print (identical in both)."""
+    return {'workload': WORKLOAD.format(keys=args.keys, queries=args.queries, dim=args.dim,
+                                        seed=args.seed),
+            'keys': args.keys, 'queries_per_gpu': args.queries, 'D': args.dim,
+            'parallelism': 'replicated mesh, queries sharded' if world > 1 else 'single GPU',
+            'l2': 'inputs larger than L2 (10M queries = 240 MB; the resident mesh about 1.6 GB)'}
+
+
 def run_reference(args, rank, world):
-    """natinterp3d's own CPU implementation (oracle/_ref) on the host cores."""
+    """natinterp3d's own CPU implementation (oracle/_ref: its C sources built with
+    its own flags) with all host threads.  Each step is get_weights + scipy
+    W @ values on a bounded sample of the workload's queries (at least 1M,
+    about 3 s of work); natinterp3d's one-time packing of its mesh and the
+    per-call set-up are warmed before timing, and the per-call set-up is
+    amortised as in a call of that size."""
     if rank != 0:
         return None
     from oracle import oracle
@@ -186,15 +207,16 @@ def run_reference(args, rank, world):
     t0 = time.perf_counter()
     ref = oracle.RefInterpolator(keys, num_threads=nthreads)
     build_s = time.perf_counter() - t0
-    # bounded sample per step: about 2 s of wall time on this host
-    probe = queries[:50_000]
+    ref.interpolate(queries[:20_000], values)  # first call packs the mesh
+    probe = queries[:200_000]
+    ref.interpolate(probe, values)
     t0 = time.perf_counter()
     ref.interpolate(probe, values)
     rate = probe.shape[0] / (time.perf_counter() - t0)
-    sample = int(min(queries.shape[0], max(50_000, rate * 2.0)))
+    sample = int(min(queries.shape[0], max(1_000_000, rate * 3.0)))
     qs = queries[:sample]
     for _ in range(max(1, args.warmup)):
-        ref.interpolate(qs[:min(sample, 100_000)], values)
+        ref.interpolate(qs, values)
     times = []
     for _ in range(args.steps):
         t0 = time.perf_counter()
@@ -206,10 +228,9 @@ def run_reference(args, rank, world):
         'impl': 'reference', 'metric': METRIC, 'value': value, 'unit': 'queries/s',
         'n_gpus': world, 'steps': args.steps, 'warmup': args.warmup,
         'ms_per_step': sec * 1e3, 'higher_is_better': True, 'scaling': 'weak',
-        'vs_baseline': None, 'dtype': 'f64', 'data': 'synthetic',
-        'config': {'workload': WORKLOAD.format(keys=args.keys, queries=args.queries, dim=args.dim,
-                                               seed=args.seed),
-                   'keys': args.keys, 'queries': args.queries, 'D': args.dim},
+        'vs_baseline': None, 'dtype': 'f64', 'data': 'synthetic: seeded uniform keys and queries, '
+                                                     'N(0,1) float32 values',
+        'config': plain_config(args, 1),
         'cpu_baseline': {'value': value, 'unit': 'queries/s', 'cores': nthreads,
                          'kind': 'reference',
                          'sample': '%d of the %d queries per step (get_weights with %d OpenMP '
@@ -277,20 +298,116 @@ def fwdbwd_cpu_baseline(interp, queries, values, gout):
                       % (n, nthreads, sec)}
 
 
-def run_fwdbwd(args, rank, world, local_rank):
-    """Differentiable workload: loss = sum(out * g), backward into queries and values."""
+def _events_ms(fn, steps, warmup):
+    import torch
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        fn()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / steps
+
+
+def _bitwise_csr(A, B):
+    return bool(np.array_equal(A.indptr, B.indptr) and np.array_equal(A.indices, B.indices) and
+                np.array_equal(np.asarray(A.data).view(np.uint8), np.asarray(B.data).view(np.uint8)))
+
+
+def _weights_leg(interp, queries, steps, warmup, cpu, sample_n, workload):
+    """get_weights on the device (count + fill, CSR left in HBM) and end to end
+    through Interpolator.get_weights (host numpy in, scipy CSR out), plus
+    natinterp3d's own get_weights on the same mesh object (all host threads)
+    on a sample, which the device rows must equal bit for bit."""
+    import ctypes
+    import torch
+    from natinterp3d_b200 import _native
+    from oracle import oracle
+    dm = interp.device_mesh
+    lib = _native.cuda_lib()
+    M = queries.shape[0]
+    qd = torch.from_numpy(queries).to(dm.device)
+    c = interp.centroid
+    step = lambda: dm.weights_csr(qd, c, vals_dtype=torch.float64)
+    ms = _events_ms(step, steps, warmup)
+    lib.nif_profile_enable(1)
+    rowptr, cols, vals, summ = dm.weights_csr(qd, c, vals_dtype=torch.float64, return_summary=True)
+    ph = (ctypes.c_double * 4)()
+    lib.nif_profile_read(ph)
+    lib.nif_profile_enable(0)
+    nnz = int(summ['nnz'])
+    del rowptr, cols, vals
+    # the CSR epilogue (row-pointer scan, then the staged rows copied into the
+    # final arrays): HBM-bound, compulsory bytes = staged rows read (4 + 8 B an
+    # entry) + final CSR written (4 + 8 B an entry) + row counts / offsets
+    epi_bytes = nnz * 24 + M * 20
+    e2e = []
+    for _ in range(2):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        W = interp.get_weights(queries)
+        e2e.append(time.perf_counter() - t0)
+    out = {'value': M / (ms * 1e-3), 'unit': 'queries/s', 'ms_per_step': ms, 'steps': steps,
+           'warmup': warmup, 'nnz': nnz,
+           'phase_ms': {'bucketing': ph[0], 'rows_fast': ph[1], 'rows_large': ph[2],
+                        'csr_epilogue': ph[3]},
+           'csr_epilogue_gbs': epi_bytes / (ph[3] * 1e-3) / 1e9 if ph[3] > 0 else None,
+           'e2e': {'value': M / e2e[-1], 'unit': 'queries/s', 'h2d_bytes_per_step': int(queries.nbytes),
+                   'd2h_bytes_per_step': int(W.data.nbytes + W.indices.nbytes + W.indptr.nbytes)},
+           'config': {'workload': workload}}
+    if cpu and oracle.ref_available() and interp.host_mesh is not None:
+        nthreads = host_threads()
+        ptr = interp.host_mesh.native_pointer()
+        qs = np.ascontiguousarray(queries[:sample_n])
+        oracle.ref_query(ptr, qs[:min(sample_n, 20_000)] - c, interp.n_keys, nthreads)  # warm
+        best = None
+        for _ in range(2):
+            t0 = time.perf_counter()
+            Wr = oracle.ref_query(ptr, qs - c, interp.n_keys, nthreads)
+            t = time.perf_counter() - t0
+            best = t if best is None else min(best, t)
+        out['bit_identical_to_natinterp3d'] = _bitwise_csr(W[:sample_n], Wr)
+        out['cpu_baseline'] = {'value': sample_n / best, 'unit': 'queries/s', 'cores': nthreads,
+                               'kind': 'reference',
+                               'sample': '%d queries of the workload: natinterp3d '
+                                         'getInsertionFreeWeightsParallel (%d threads) on the same '
+                                         'mesh, best of 2, %.2f s' % (sample_n, nthreads, best)}
+    return out
+
+
+def leg_get_weights_small(local_rank, steps, warmup, cpu=True):
+    """get_weights at the small configuration: 10,000 keys U[0,1]^3, 100,000
+    queries U[0.05,0.95]^3, seed 0 (float64)."""
+    import torch
+    import natinterp3d_b200 as ni
+    dev = torch.device('cuda', local_rank)
+    rng = np.random.default_rng(0)
+    keys = rng.uniform(0.0, 1.0, (10_000, 3))
+    queries = rng.uniform(0.05, 0.95, (100_000, 3))
+    interp = ni.Interpolator(keys, device=dev, keep_host_mesh=cpu)
+    return _weights_leg(interp, queries, steps, warmup, cpu, 100_000,
+                        'get_weights: 10,000 keys U[0,1]^3, 100,000 queries U[0.05,0.95]^3, '
+                        'float64, seed 0')
+
+
+def leg_fwdbwd(args, rank, local_rank, steps, warmup, cpu=True):
+    """Differentiable workload: loss = sum(out * g), backward into queries and
+    values (200k keys U[0,1]^3, 1M queries U[0.1,0.9]^3 float64 with grad,
+    values D=16 float32 with grad, seed 3)."""
     import torch
     import natinterp3d_b200 as ni
     from natinterp3d_b200 import autograd as nag
-    keys_n = 200_000 if args.keys == 1_000_000 else args.keys
-    q_n = 1_000_000 if args.queries == 10_000_000 else args.queries
-    dim = 16 if args.dim == 3 else args.dim
+    keys_n, q_n, dim = 200_000, 1_000_000, 16
     torch.cuda.set_device(local_rank)
     dev = torch.device('cuda', local_rank)
     rng = np.random.default_rng([3, rank])
     keys = rng.uniform(0, 1, (keys_n, 3))
-    interp = ni.Interpolator(keys, device=dev,
-                             keep_host_mesh=(rank == 0 and not args.no_cpu_baseline))
+    t0 = time.perf_counter()
+    interp = ni.Interpolator(keys, device=dev, keep_host_mesh=cpu)
+    build_s = time.perf_counter() - t0
     qn = rng.uniform(0.1, 0.9, (q_n, 3))
     vn = rng.standard_normal((keys_n, dim)).astype(np.float32)
     gn = rng.standard_normal((q_n, dim))
@@ -313,31 +430,38 @@ def run_fwdbwd(args, rank, world, local_rank):
         return q.grad, v.grad
 
     def timed(fn):
-        for _ in range(args.warmup):
+        for _ in range(warmup):
             fn()
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
-        for _ in range(args.steps):
+        for _ in range(steps):
             fn()
         e1.record()
         torch.cuda.synchronize()
-        return e0.elapsed_time(e1) / args.steps
+        return e0.elapsed_time(e1) / steps
 
     ms_fwd = timed(fwd)
     ms_fb = timed(fwdbwd)
-    cpu = None if (args.no_cpu_baseline or rank != 0) else fwdbwd_cpu_baseline(interp, qn, vn, gn)
+    base = fwdbwd_cpu_baseline(interp, qn, vn, gn) if cpu else None
+    return {
+        'metric': METRIC, 'mode': 'fwd+bwd', 'value': q_n / (ms_fb * 1e-3), 'unit': 'queries/s',
+        'steps': steps, 'warmup': warmup, 'ms_per_step': ms_fb,
+        'plain_forward_ms': ms_fwd, 'fwdbwd_over_forward': ms_fb / ms_fwd, 'cpu_baseline': base,
+        'higher_is_better': True, 'dtype': 'f64', 'data': 'synthetic',
+        'config': {'workload': 'differentiable: %d keys U[0,1]^3, %d queries U[0.1,0.9]^3 float64 '
+                               'with grad, values D=%d float32 with grad, loss=sum(out*g), seed 3'
+                               % (keys_n, q_n, dim)},
+        'setup': {'mesh_build_s': round(build_s, 2), 'tuning': interp.tuning,
+                  'autotuned': tuned is not None}}
+
+
+def run_fwdbwd(args, rank, world, local_rank):
+    line = leg_fwdbwd(args, rank, local_rank, args.steps, args.warmup,
+                      cpu=(rank == 0 and not args.no_cpu_baseline))
     if rank == 0:
-        print(json.dumps({
-            'metric': METRIC, 'mode': 'fwd+bwd', 'value': q_n / (ms_fb * 1e-3), 'unit': 'queries/s',
-            'n_gpus': world, 'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': ms_fb,
-            'plain_forward_ms': ms_fwd, 'fwdbwd_over_forward': ms_fb / ms_fwd,
-            'cpu_baseline': cpu,
-            'higher_is_better': True, 'dtype': 'f64', 'data': 'synthetic',
-            'config': {'workload': 'differentiable: %d keys U[0,1]^3, %d queries U[0.1,0.9]^3 float64 '
-                                   'with grad, values D=%d float32 with grad, loss=sum(out*g), seed 3'
-                                   % (keys_n, q_n, dim),
-                       'tuning': interp.tuning, 'autotuned': tuned is not None}}))
+        line['n_gpus'] = world
+        print(json.dumps(line))
 
 
 def batched_workload(P, seed):
@@ -354,7 +478,7 @@ def batched_workload(P, seed):
     return keys, queries, values
 
 
-def run_batched(args, rank, world, local_rank):
+def leg_batched(args, rank, local_rank, steps, warmup, cpu=True):
     """Uneven batch: one captured graph vs one plain call per problem vs natinterp3d's loop."""
     import torch
     from natinterp3d_b200.batch import BatchInterpolator
@@ -380,16 +504,16 @@ def run_batched(args, rank, world, local_rank):
     same = bool(torch.equal(graph.replay(), eager))
 
     def timed(fn):
-        for _ in range(args.warmup):
+        for _ in range(warmup):
             fn()
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
-        for _ in range(args.steps):
+        for _ in range(steps):
             fn()
         e1.record()
         torch.cuda.synchronize()
-        return e0.elapsed_time(e1) / args.steps
+        return e0.elapsed_time(e1) / steps
 
     ms_graph = timed(graph.replay)
     ms_loop = timed(lambda: b.interpolate_per_problem(qcat, qoff, vcat))
@@ -414,8 +538,8 @@ def run_batched(args, rank, world, local_rank):
         t0 = time.perf_counter()
         b.interpolate(queries, values)
         host_batch_s = time.perf_counter() - t0
-    cpu = None
-    if rank == 0 and oracle.ref_available():
+    base = None
+    if cpu and oracle.ref_available():
         # natinterp3d's own code, one Interpolator per problem, on a sample of problems
         nthreads = host_threads()
         sample = list(range(0, args.problems, max(1, args.problems // 24)))
@@ -425,25 +549,32 @@ def run_batched(args, rank, world, local_rank):
             r.interpolate(queries[p], values[p])
         sec = time.perf_counter() - t0
         nq = sum(len(queries[p]) for p in sample)
-        cpu = {'value': nq / sec, 'unit': 'queries/s', 'cores': nthreads, 'kind': 'reference',
+        base = {'value': nq / sec, 'unit': 'queries/s', 'cores': nthreads, 'kind': 'reference',
                'sample': '%d of %d problems (%d queries): natinterp3d Interpolator per problem, '
                          'get_weights + scipy W @ values' % (len(sample), args.problems, nq)}
+    return {
+        'metric': METRIC, 'mode': 'batched', 'value': M / (ms_graph * 1e-3), 'unit': 'queries/s',
+        'steps': steps, 'warmup': warmup, 'ms_per_step': ms_graph,
+        'per_problem_launches_ms': ms_loop, 'batched_over_per_problem_speedup': ms_loop / ms_graph,
+        'per_problem_api_ms': ms_api, 'batched_over_per_problem_api': ms_api / ms_graph,
+        'host_api_per_problem_s': host_loop_s, 'host_api_batched_s': host_batch_s,
+        'host_api_speedup': host_loop_s / host_batch_s,
+        'bit_identical_to_per_problem': same, 'higher_is_better': True, 'dtype': 'f64',
+        'data': 'synthetic', 'cpu_baseline': base,
+        'config': {'workload': '%d problems, keys log-uniform [500, 100k] in boxes of side 0.5-2, '
+                               'queries log-uniform [1k, 200k] in the boxes shrunk 5%%, values D=4 '
+                               'float32, seed 4' % args.problems,
+                   'total_keys': int(b.n_keys.sum()), 'total_queries': M},
+        'setup': {'mesh_build_s': round(build_s, 1), 'tuning': b.get_tuning(),
+                  'autotuned': tuned is not None}}
+
+
+def run_batched(args, rank, world, local_rank):
+    line = leg_batched(args, rank, local_rank, args.steps, args.warmup,
+                       cpu=(rank == 0 and not args.no_cpu_baseline))
     if rank == 0:
-        print(json.dumps({
-            'metric': METRIC, 'mode': 'batched', 'value': M / (ms_graph * 1e-3), 'unit': 'queries/s',
-            'n_gpus': world, 'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': ms_graph,
-            'per_problem_launches_ms': ms_loop, 'batched_over_per_problem_speedup': ms_loop / ms_graph,
-            'per_problem_api_ms': ms_api, 'batched_over_per_problem_api': ms_api / ms_graph,
-            'host_api_per_problem_s': host_loop_s, 'host_api_batched_s': host_batch_s,
-            'host_api_speedup': host_loop_s / host_batch_s,
-            'bit_identical_to_per_problem': same, 'higher_is_better': True, 'dtype': 'f64',
-            'data': 'synthetic', 'cpu_baseline': cpu,
-            'config': {'workload': '%d problems, keys log-uniform [500, 100k] in boxes of side 0.5-2, '
-                                   'queries log-uniform [1k, 200k] in the boxes shrunk 5%%, values D=4 '
-                                   'float32, seed 4' % args.problems,
-                       'total_keys': int(b.n_keys.sum()), 'total_queries': M,
-                       'mesh_build_s': round(build_s, 1), 'tuning': b.get_tuning(),
-                       'autotuned': tuned is not None}}))
+        line['n_gpus'] = world
+        print(json.dumps(line))
 
 
 def main():
@@ -523,7 +654,6 @@ def main():
     if dist is not None:
         dist.barrier()
     lib.nif_profile_enable(1)
-    kernel_ms = []
     with ClockSampler(local_rank) as clocks:
         torch.cuda.synchronize()
         e0 = torch.cuda.Event(enable_timing=True)
@@ -531,11 +661,12 @@ def main():
         e0.record()
         for _ in range(args.steps):
             step()
-            ph = (ctypes.c_double * 4)()
-            if lib.nif_profile_read(ph) == 0:
-                kernel_ms.append(list(ph))
         e1.record()
         torch.cuda.synchronize()
+    # per-phase device times of the timed calls (events recorded in each call,
+    # read once here: the loop itself never waits on the host)
+    ph = (ctypes.c_double * 4)()
+    have_phases = lib.nif_profile_read(ph) == 0
     lib.nif_profile_enable(0)
     ms = e0.elapsed_time(e1) / args.steps
     if dist is not None:
@@ -561,8 +692,8 @@ def main():
         e2e_sec = float(t.item())
 
     if rank == 0:
-        kms = np.array(kernel_ms) if kernel_ms else np.zeros((1, 4))
-        rows_ms = float(np.mean(kms[:, 1]))
+        phases = list(ph) if have_phases else [0.0] * 4
+        rows_ms = phases[1]
         fpq = flops_per_query(stats, summ['walk_steps'], M)
         fused, separate = ctypes.c_double(), ctypes.c_double()
         lib.nif_measure_fp64_peak(ctypes.byref(fused), ctypes.byref(separate))
@@ -573,16 +704,12 @@ def main():
             'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': ms,
             'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f64',
             'data': 'synthetic: seeded uniform keys and queries, N(0,1) float32 values',
-            'config': {
-                'workload': WORKLOAD.format(keys=args.keys, queries=args.queries, dim=args.dim,
-                                            seed=args.seed),
-                'keys': args.keys, 'queries_per_gpu': args.queries, 'D': args.dim,
-                'parallelism': 'replicated mesh, queries sharded' if world > 1 else 'single GPU',
-                'l2': 'inputs larger than L2 (queries %.0f MB, resident mesh %.0f MB)'
-                      % (queries.nbytes / 1e6, dm.nbytes / 1e6),
+            'config': plain_config(args, world),
+            'setup': {
                 'mesh_build_s': round(build_s, 2), 'mesh_upload_s': round(upload_s, 3),
-                'tets': dm.n_tets, 'bit_identical_to_oracle_on_sample': exact,
-                'predicates': args.predicates,
+                'tets': dm.n_tets, 'resident_mesh_mb': round(dm.nbytes / 1e6, 1),
+                'octree': dm.octree_stats,
+                'bit_identical_to_oracle_on_sample': exact, 'predicates': args.predicates,
                 'tuning': dm.get_tuning(), 'autotuned': tuned is not None,
                 'tune_s': round(tune_s, 2), 'tune_sample_ms': tune_times,
             },
@@ -594,14 +721,13 @@ def main():
                 'peak_note': 'measured on this GPU by nif_measure_fp64_peak: separately rounded '
                              'DMUL+DADD (the kernels never fuse, for bit parity)',
                 'flops_per_query': fpq, 'kernel_ms': rows_ms,
-                'phase_ms': {'bucketing': float(np.mean(kms[:, 0])), 'rows_fast': rows_ms,
-                             'rows_large': float(np.mean(kms[:, 2])),
-                             'epilogue': float(np.mean(kms[:, 3]))},
-                # dram__bytes_read.sum + dram__bytes_write.sum of one full-size k_rows_fast
-                # launch (1M keys, 10M queries, tuning 8,0,8; profiles/launches_1M_keys_10M_queries.md),
-                # scaled by this launch's query count
-                'traffic': 4.4257e9 * (M / 10_000_000),
-                'traffic_note': 'ncu capture of one k_rows_fast launch at 1M keys / 10M queries',
+                'phase_ms': {'bucketing': phases[0], 'rows_fast': rows_ms,
+                             'rows_large': phases[2], 'epilogue': phases[3]},
+                # dram__bytes_read.sum + dram__bytes_write.sum of one k_rows_fast
+                # launch from an ncu capture of this workload (profiles/), scaled
+                # by this launch's query count
+                'traffic': TRAFFIC_PER_QUERY * M,
+                'traffic_note': 'ncu capture of one k_rows_fast launch, %s' % TRAFFIC_SOURCE,
             },
             'cpu_baseline': cpu,
             'e2e': {'value': M * world / e2e_sec, 'unit': 'queries/s',
@@ -609,8 +735,24 @@ def main():
                     'd2h_bytes_per_step': int(out.nbytes)},
             'gpu_launches': 7 * args.steps,
             'clocks': clocks.summary(),
-            'summary': {k: int(v) for k, v in summ.items()},
+            'summary': {k: int(v) for k, v in summ.items() if k != 'nnz'},
         }
+        if world == 1 and not args.no_legs:
+            # the other legs of the metric, each with its own CPU baseline
+            cpu_on = not args.no_cpu_baseline
+            legs = {}
+            legs['get_weights_1M_keys_10M_queries'] = _weights_leg(
+                interp, queries, 3, 1, cpu_on, 1_000_000,
+                'get_weights on the plain workload: ' + WORKLOAD.format(
+                    keys=args.keys, queries=args.queries, dim=args.dim, seed=args.seed))
+            legs['get_weights_10k_keys_100k_queries'] = leg_get_weights_small(
+                local_rank, max(args.steps, 5), 3, cpu_on)
+            del out
+            legs['fwd+bwd'] = leg_fwdbwd(args, rank, local_rank, max(args.steps, 5),
+                                         max(args.warmup, 3), cpu_on)
+            legs['batched'] = leg_batched(args, rank, local_rank, max(args.steps, 3),
+                                          max(args.warmup, 3), cpu_on)
+            line['legs'] = legs
         print(json.dumps(line))
     if dist is not None:
         dist.barrier()

@@ -33,7 +33,7 @@ extern "C" {
 #define NIF_ERR_INTERNAL (-4)   /* inconsistent mesh / internal check failed */
 #define NIF_ERR_OVERFLOW (-5)   /* nnz > INT32_MAX; natinterp3d returns -1 here,
                                    natural_insertionfree.c:901-912, and Python
-                                   raises OverflowError (natinterp3d_cython.pyx:278-280) */
+                                   raises OverflowError (natinterp3d_cython.pyx:86-88, 129-131) */
 #define NIF_ERR_WALK (-6)       /* a point-location walk exceeded its step limit
                                    (natinterp3d's walk, delaunay.c:398-405, has none) */
 #define NIF_ERR_CUDA (-7)       /* a CUDA runtime call failed */
@@ -46,7 +46,8 @@ extern "C" {
 #define NIF_F32 1
 
 /* ---- workspace modes --------------------------------------------------- */
-#define NIF_MODE_WEIGHTS 0      /* get_weights: rows are staged, then compacted to CSR */
+#define NIF_MODE_WEIGHTS 0      /* get_weights: rows are counted (and short ones staged), then
+                                   written to the CSR */
 #define NIF_MODE_INTERP 1       /* interpolate: rows are reduced against values in place */
 
 /* ======================================================================== */
@@ -57,8 +58,8 @@ typedef struct nif_mesh nif_mesh;
 
 /* Builds natinterp3d's Delaunay tetrahedralization of n centred keys
  * ([n][3] float64).  Replaces buildNewMeshAndVertices (natural.h:16,
- * natural.c:114-118) as called from natinterp3d_cython.pyx:105-106 and
- * :254-256.  Returns NIF_ERR_DEGENERATE where natinterp3d would exit(1)
+ * natural.c:114-118) as called from natinterp3d_cython.pyx:64-65 and
+ * :106-107.  Returns NIF_ERR_DEGENERATE where natinterp3d would exit(1)
  * (zero or non-finite extent along an axis). */
 int nif_mesh_build(const double *keys_centered, int n, nif_mesh **out);
 
@@ -90,8 +91,10 @@ typedef struct nif_dmesh nif_dmesh;
 
 /* Size in bytes of the device buffer that holds a resident mesh of
  * n_vertices (= keys + 4) and n_tets (at most 2^29 - 1) tets: vertices, tets, neighbours,
- * orientation and mirror flags, cached tet and face circumcentres and the
- * point-location seed grid.  (natinterp3d keeps the mesh as pointer-linked
+ * orientation and mirror flags, cached tet and face circumcentres, and the
+ * tet centroids with an octree over them for the point-location seed (the
+ * nearest tet centroid, which natinterp3d finds in a k-d tree built by its
+ * constructor, delaunay.c:141-159).  (natinterp3d keeps the mesh as pointer-linked
  * structs, delaunay.h:44-70, and re-packs it on first query,
  * natural_insertionfree.c:397-450.) */
 int nif_dmesh_bytes(int n_vertices, int n_tets, size_t *bytes);
@@ -109,8 +112,8 @@ int nif_dmesh_create(const double *d_vxyz, const int32_t *d_tet_v, const int32_t
 /* Frees the host handle (the device buffer belongs to the caller). */
 void nif_dmesh_destroy(nif_dmesh *m);
 
-/* Seed-grid dimensions, tet/vertex counts and the predicate state:
- * info = {n_vertices, n_tets, grid_x, grid_y, grid_z, orient_uncertain,
+/* Tet/vertex counts, the centroid octree's size and the predicate state:
+ * info = {n_vertices, n_tets, octree_nodes, octree_levels, 0, orient_uncertain,
  *         orient_flipped, predicate_mode}, where orient_uncertain counts the
  * tets whose orient3dfast sign (natural_insertionfree.c:457-476) the static
  * error bound cannot certify and orient_flipped those whose "> 0" flag the
@@ -195,19 +198,27 @@ int nif_query_workspace_bytes(const nif_dmesh *m, int64_t M, int mode, size_t *b
  * and writes d_rowptr (int32[M+1]).  Synchronises `stream` and fills
  * *summary.  Returns NIF_ERR_OVERFLOW (d_rowptr untouched) when
  * nnz > INT32_MAX.  Replaces getInsertionFreeWeightsParallel
- * (natural_insertionfree.h:103-106) up to its row-pointer pass
+ * (natural_insertionfree.h:81-84) up to its row-pointer pass
  * (natural_insertionfree.c:896-913). */
 int nif_weights_count(const nif_dmesh *m, const void *d_queries, int query_dtype, int64_t M,
                       const double centroid[3], void *d_ws, size_t ws_bytes, int32_t *d_rowptr,
                       void *stream, nif_summary *summary);
 
-/* Sibson weights, step 2 of 2: copies the rows staged by nif_weights_count
- * into CSR arrays d_vals (vals_dtype, nnz) and d_cols (int32, nnz).  Columns
- * of a row appear in natinterp3d's first-seen order.  If d_row_totals is not
- * NULL it receives each row's normaliser (the sum of its stolen volumes, 0
- * for empty rows; float64 [M]), which nif_query_grad takes as input.  Replaces the CSR copy
- * of natural_insertionfree.c:915-928 (natinterp3d mallocs vals/cols itself). */
-int nif_weights_fill(const nif_dmesh *m, int64_t M, const void *d_ws, size_t ws_bytes,
+/* Sibson weights, step 2 of 2: writes the CSR arrays d_vals (vals_dtype,
+ * nnz) and d_cols (int32, nnz) for the d_rowptr of step 1.  Takes the same
+ * queries, dtype, M, centroid and workspace as nif_weights_count (the queries
+ * must be unchanged in between).  Rows of up to 24 entries were staged by
+ * step 1 and are copied; longer rows, and rows the large-capacity kernel
+ * handled, are recomputed straight into their slices, so the workspace holds
+ * no more than 24 entries a row and no row is limited by a staging arena.
+ * Columns of a row appear in natinterp3d's first-seen order.  If
+ * d_row_totals is not NULL it receives each row's normaliser (the sum of its
+ * stolen volumes, 0 for empty rows; float64 [M]), which nif_query_grad takes
+ * as input.  Replaces the CSR copy of natural_insertionfree.c:915-928
+ * (natinterp3d mallocs vals/cols itself, and grows per-thread arenas while
+ * it computes, natural_insertionfree.c:750). */
+int nif_weights_fill(const nif_dmesh *m, const void *d_queries, int query_dtype, int64_t M,
+                     const double centroid[3], const void *d_ws, size_t ws_bytes,
                      const int32_t *d_rowptr, void *d_vals, int vals_dtype, int32_t *d_cols,
                      double *d_row_totals, void *stream);
 
@@ -298,10 +309,11 @@ int nif_batch_summary(const nif_dbatch *b, int64_t total_queries, const void *d_
                       void *stream, nif_summary *summary);
 
 /* Measurement.  While enabled, every query call records CUDA events on its
- * stream between its phases; nif_profile_read waits for the last call's
- * final event and returns the device time in milliseconds of
- * {query bucketing, shared-memory row kernel, large-row kernel, CSR scan or
- * epilogue} of that call.  (natinterp3d has no counterpart.) */
+ * stream between its phases (no host synchronisation); nif_profile_read
+ * waits for the last complete call and returns the device time in
+ * milliseconds of {query bucketing, shared-memory row kernel, large-row
+ * kernel, CSR scan or epilogue}, averaged over the calls since the last
+ * enable or read (at most the last 64).  (natinterp3d has no counterpart.) */
 int nif_profile_enable(int on);
 int nif_profile_read(double ms[4]);
 
@@ -325,7 +337,10 @@ int nif_measure_fp64_peak(double *tflops_fused, double *tflops_separate);
  * queries per call; more return NIF_ERR_TOO_LARGE (split the batch).
  * The mesh's device must be current.  The first call on each device looks up
  * the array's device address (a CUDA runtime query, made once per device);
- * make that first call before any stream capture.  All calls share the one
+ * make that first call before any stream capture.  That address belongs to
+ * the runtime's primary context of the device: call from that context (not a
+ * context the caller created with the driver API), and not after a
+ * cudaDeviceReset in the same process.  All calls share the one
  * array and each call re-initialises what must start at zero, so two calls
  * that can run on the GPU at the same time (different streams, or different
  * host threads) race on it: serialise them.  Allocates no device or host

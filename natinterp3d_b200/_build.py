@@ -27,7 +27,10 @@ LIB_DIR = os.path.join(PKG_DIR, 'lib')
 INCLUDE_DIR = os.path.join(REPO_DIR, 'include')
 MESH_SO = os.path.join(LIB_DIR, 'libnif_mesh.so')
 CUDA_SO = os.path.join(LIB_DIR, 'libnif_cuda.so')
-DEFAULT_REF_SRC = '/root/reference/src/natinterp3d'
+# Where this recipe looks for natinterp3d's C sources, in order: the
+# NATINTERP3D_SRC environment variable; an importable natinterp3d package
+# whose directory holds them; the source checkout this build reads by default.
+CHECKOUT_REF_SRC = '/root/reference/src/natinterp3d'
 
 # natinterp3d's Linux compile flags (setup.py:17-22, 36 of natinterp3d)
 MESH_CFLAGS = ['-std=c11', '-O3', '-fno-math-errno', '-flto', '-fopenmp',
@@ -40,8 +43,26 @@ NVCC_FLAGS = ['-O3', '-std=c++17', '-gencode', 'arch=compute_100a,code=sm_100a',
               '-Xcompiler', '-fvisibility=hidden', '-cudart', 'static', '--expt-relaxed-constexpr']
 
 
+def _has_sources(d):
+    return bool(d) and os.path.exists(os.path.join(d, 'delaunay.c'))
+
+
 def ref_source_dir():
-    return os.environ.get('NATINTERP3D_SRC', DEFAULT_REF_SRC)
+    """Directory of natinterp3d's C sources (may not exist where only the
+    prebuilt libraries travel)."""
+    env = os.environ.get('NATINTERP3D_SRC')
+    if env:
+        return env
+    try:
+        import importlib.util
+        spec = importlib.util.find_spec('natinterp3d')
+        if spec is not None and spec.origin:
+            d = os.path.dirname(spec.origin)
+            if _has_sources(d):
+                return d
+    except (ImportError, ValueError):
+        pass
+    return CHECKOUT_REF_SRC
 
 
 def _cc():

@@ -167,6 +167,14 @@ class Summary(ctypes.Structure):
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_ if k != 'reserved'}
 
+    @classmethod
+    def from_dict(cls, d):
+        s = cls()
+        for k, _ in cls._fields_:
+            if k in d:
+                setattr(s, k, int(d[k]))
+        return s
+
 
 class Tuning(ctypes.Structure):
     """nif_tuning: launch settings of the query kernels (speed only, never results)."""
@@ -195,8 +203,8 @@ CUDA_SIGNATURES = {
     'nif_query_workspace_bytes': (c_int, [c_void_p, c_int64, c_int, ctypes.POINTER(c_size_t)]),
     'nif_weights_count': (c_int, [c_void_p, c_void_p, c_int, c_int64, c_double_p, c_void_p,
                                   c_size_t, c_void_p, c_void_p, ctypes.POINTER(Summary)]),
-    'nif_weights_fill': (c_int, [c_void_p, c_int64, c_void_p, c_size_t, c_void_p, c_void_p, c_int,
-                                 c_void_p, c_void_p, c_void_p]),
+    'nif_weights_fill': (c_int, [c_void_p, c_void_p, c_int, c_int64, c_double_p, c_void_p, c_size_t,
+                                 c_void_p, c_void_p, c_int, c_void_p, c_void_p, c_void_p]),
     'nif_interpolate': (c_int, [c_void_p, c_void_p, c_int, c_int64, c_double_p, c_void_p, c_int,
                                 c_int, c_void_p, c_int, c_void_p, c_size_t, c_void_p,
                                 ctypes.POINTER(Summary)]),

@@ -103,11 +103,13 @@ class BatchInterpolator:
             _vp(self.key_offsets), D, _vp(out), _DT[out.dtype], int(q.shape[0]), _vp(ws), ws.numel(),
             _stream_ptr(self.device)), 'nif_batch_interpolate')
 
-    def summary(self, total_queries, ws):
+    def summary(self, total_queries, ws, stream=None):
+        """Row counters of the last batch call on ``ws``, read through
+        ``stream`` (default: the current stream), the only stream it waits for."""
         s = N.Summary()
-        N.check(self._lib.nif_batch_summary(self._h, int(total_queries), _vp(ws), ws.numel(),
-                                            _stream_ptr(self.device), ctypes.byref(s)),
-                'nif_batch_summary')
+        sp = ctypes.c_void_p(stream.cuda_stream) if stream is not None else _stream_ptr(self.device)
+        N.check(self._lib.nif_batch_summary(self._h, int(total_queries), _vp(ws), ws.numel(), sp,
+                                            ctypes.byref(s)), 'nif_batch_summary')
         return s
 
     def _prepare(self, q, qoff, v):
@@ -186,7 +188,10 @@ class BatchInterpolator:
         ostage = [torch.empty((cap, D), dtype=odt, pin_memory=True) for _ in range(2)]
         with torch.cuda.device(dev):
             vd = torch.empty((int(ko[-1]), D), dtype=vdt, device=dev)
-            pending, checks = None, []
+            # two workspaces in turn: a group's counters are read (on the copy
+            # stream) before the group two later reuses its workspace
+            wss = [self.workspace(cap) for _ in range(2)]
+            pending, counters = None, []
 
             def drain(item):
                 slot, (a, b), res, done = item
@@ -196,6 +201,7 @@ class BatchInterpolator:
                     res.record_stream(copy)
                 copy.synchronize()
                 out[a:b] = ostage[slot][:b - a].numpy()
+                counters.append(self.summary(b - a, wss[slot], stream=copy))
 
             for k, (g0, g1) in enumerate(groups):
                 a, b = int(qoff[g0]), int(qoff[g1])
@@ -216,9 +222,7 @@ class BatchInterpolator:
                 qd.record_stream(compute)
                 gd.record_stream(compute)
                 res = torch.empty((b - a, D), dtype=odt, device=dev)
-                ws = self.workspace(b - a)
-                self._launch(qd, gd, vd, res, ws)
-                checks.append((b - a, ws))
+                self._launch(qd, gd, vd, res, wss[slot])
                 done = torch.cuda.Event()
                 done.record(compute)
                 if pending is not None:
@@ -226,8 +230,8 @@ class BatchInterpolator:
                     # the staging slot of the drained group is free again
                 pending = (slot, (a, b), res, done)
             drain(pending)
-            for n, ws in checks:
-                DeviceMesh._raise_rows(self.summary(n, ws))
+            for summ in counters:
+                DeviceMesh._raise_rows(summ)
         return out
 
     def interpolate_per_problem(self, queries, query_offsets, values):

@@ -55,7 +55,7 @@ constexpr int FAST_G = NIF_FAST_G;    // lanes per query in the shared-memory ke
 using FastWS = Workspace<256, 96, 128, 64, 128, FAST_G, uint8_t, int8_t>;
 constexpr int LARGE_G = 32;
 using LargeWS = Workspace<16384, 4096, 8192, 2048, 8192, LARGE_G, uint16_t, int16_t>;
-constexpr int ROW_CAP = FastWS::NBR;  // staged entries per row
+constexpr int ROW_STAGE = 24;         // get_weights: entries staged per row (mean about 15.5)
 
 constexpr int FAST_BLOCK = 128;       // 4 warps
 constexpr int LARGE_GROUPS = 64;      // concurrent large-row groups (one warp each)
@@ -75,7 +75,7 @@ struct DevSummary {
     unsigned long long walk_steps;
     int first_status;
     int large_count;  // rows queued for the large kernel
-    unsigned long long arena_used;
+    int refill_count; // get_weights: fast-kernel rows longer than ROW_STAGE
     // predicate evaluations the filter could not certify / whose decision the
     // exact sign changes (PRED_AUDIT and PRED_EXACT meshes)
     unsigned long long orient_unc, orient_flip, insphere_unc, insphere_flip;
@@ -215,42 +215,136 @@ __global__ void k_bbox_partial(const d4 *__restrict__ vtx, int n, double *__rest
         for (int a = 0; a < 6; a++) part[6 * blockIdx.x + a] = s[a][0];
 }
 
-// Seed grid, built coarse to fine: the tet of every cell of level k is found
-// by walking from its parent cell's tet to the cell centre.
-__global__ void k_seed_level(MeshView M, int dx, int dy, int dz, int pdx, int pdy, int pdz,
-                             const int *__restrict__ parent, int *__restrict__ out, int *__restrict__ bad) {
-    const int ncell = dx * dy * dz;
-    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < ncell; c += gridDim.x * blockDim.x) {
-        const int x = c % dx, y = (c / dx) % dy, z = c / (dx * dy);
-        int t = 0;
-        if (parent) {
-            const int px = (pdx == dx) ? x : x >> 1;
-            const int py = (pdy == dy) ? y : y >> 1;
-            const int pz = (pdz == dz) ? z : z >> 1;
-            t = parent[(pz * pdy + py) * pdx + px];
+__device__ __forceinline__ unsigned spread3(unsigned v) {  // 10 bits -> every third bit
+    v &= 0x3ffu;
+    v = (v | (v << 16)) & 0x030000ffu;
+    v = (v | (v << 8)) & 0x0300f00fu;
+    v = (v | (v << 4)) & 0x030c30c3u;
+    v = (v | (v << 2)) & 0x09249249u;
+    return v;
+}
+
+// Centroid of tet p as natinterp3d's constructor computes it for its k-d tree
+// (delaunay.c:151-157): (p0 + p1 + p2 + p3) / 4 per axis, summed left to right.
+__device__ __forceinline__ d4 tet_centroid(const MeshView &M, const int4 &p, int t) {
+    const d4 a = M.vtx[p.x], b = M.vtx[p.y], c = M.vtx[p.z], d = M.vtx[p.w];
+    return d4{fdiv(fadd(fadd(fadd(a.x, b.x), c.x), d.x), 4.0),
+              fdiv(fadd(fadd(fadd(a.y, b.y), c.y), d.y), 4.0),
+              fdiv(fadd(fadd(fadd(a.z, b.z), c.z), d.z), 4.0), (double)t};
+}
+
+// 60-bit Morton code of each tet centroid's cell (oct_code), split into two
+// 32-bit words for the radix sort (low word first, then the high word)
+__global__ void k_cen_code(MeshView M, uint32_t *__restrict__ chi, uint32_t *__restrict__ clo,
+                           uint32_t *__restrict__ key, int32_t *__restrict__ idx) {
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < M.nt; t += gridDim.x * blockDim.x) {
+        const d4 c = tet_centroid(M, M.tv[t], t);
+        int ix[3];
+        const unsigned long long code = oct_code(M, dv3{c.x, c.y, c.z}, ix);
+        chi[t] = (uint32_t)(code >> 32);
+        clo[t] = (uint32_t)code;
+        key[t] = (uint32_t)code;
+        idx[t] = t;
+    }
+}
+
+__global__ void k_gather_key(const uint32_t *__restrict__ src, const int32_t *__restrict__ idx, int n,
+                             uint32_t *__restrict__ key) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
+        key[k] = src[idx[k]];
+}
+
+__global__ void k_cen_gather(MeshView M, const int32_t *__restrict__ idx, const uint32_t *__restrict__ chi,
+                             const uint32_t *__restrict__ clo, d4 *__restrict__ cs,
+                             unsigned long long *__restrict__ code) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < M.nt; k += gridDim.x * blockDim.x) {
+        const int t = idx[k];
+        cs[k] = tet_centroid(M, M.tv[t], t);
+        code[k] = ((unsigned long long)chi[t] << 32) | clo[t];
+    }
+}
+
+// Octree build, one node level at a time.  Nodes are numbered level by level
+// in centroid order; node j spans centroids [na[j], nb[j]).  node_of[i] is
+// the deepest node built so far that holds centroid i.  A level-k node with
+// more than OCT_SPLIT centroids gets one child per distinct 6-bit digit k of
+// its centroids' codes: flag marks each child's first centroid.
+__device__ __forceinline__ bool oct_splits(const int *na, const int *nb, int p, int s0, int s1) {
+    return p >= s0 && p < s1 && nb[p] - na[p] > OCT_SPLIT;
+}
+
+__global__ void k_oct_flag(const unsigned long long *__restrict__ code, int nt, const int *__restrict__ node_of,
+                           const int *__restrict__ na, const int *__restrict__ nb, int s0, int s1, int k,
+                           int *__restrict__ flag) {
+    const int sh = 6 * (OCT_KMAX - 1 - k);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nt; i += gridDim.x * blockDim.x) {
+        const int p = node_of[i];
+        int f = 0;
+        if (oct_splits(na, nb, p, s0, s1))
+            f = (i == na[p]) || ((code[i] >> sh) != (code[i - 1] >> sh));
+        flag[i] = f;
+    }
+}
+
+__global__ void k_oct_link(const unsigned long long *__restrict__ code, int nt, int *__restrict__ node_of,
+                           int *__restrict__ na, const int *__restrict__ nb, int s0, int s1, int k,
+                           const int *__restrict__ flag, const int *__restrict__ scan, int *__restrict__ par,
+                           int *__restrict__ first, int *__restrict__ nch, unsigned long long *__restrict__ mask) {
+    const int sh = 6 * (OCT_KMAX - 1 - k);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nt; i += gridDim.x * blockDim.x) {
+        const int p = node_of[i];
+        if (!oct_splits(na, nb, p, s0, s1)) continue;
+        const int f = flag[i];
+        if (f) {
+            const int j = s1 + scan[i];
+            na[j] = i;
+            par[j] = p;
+            if (i == na[p]) first[p] = j;
+            atomicAdd(&nch[p], 1);
+            atomicOr(&mask[p], 1ull << (int)((code[i] >> sh) & 63ull));
         }
-        // centre of the cell: the finest grid has gdim cells of 1/ginv per axis,
-        // this level has d cells of gdim/(d*ginv)
-        const dv3 q = mk(M.glo[0] + (x + 0.5) * (double)M.gdim[0] / (dx * M.ginv[0]),
-                         M.glo[1] + (y + 0.5) * (double)M.gdim[1] / (dy * M.ginv[1]),
-                         M.glo[2] + (z + 0.5) * (double)M.gdim[2] / (dz * M.ginv[2]));
-        const int t0 = t;
-        for (int step = 0; step < (1 << 22); step++) {
-            const int4 p = M.tv[t];
-            int f = 0;
-            for (; f < 4; f++) {
-                const dv3 v1 = vload(M, comp(p, face_vslot(f, 0)));
-                const dv3 v2 = vload(M, comp(p, face_vslot(f, 1)));
-                const dv3 v3 = vload(M, comp(p, face_vslot(f, 2)));
-                if (orient_fast(v1, v2, v3, q) < 0) break;
+        node_of[i] = s1 + scan[i] + f - 1;
+    }
+}
+
+__global__ void k_oct_end(int s1, int T, const int *__restrict__ na, const int *__restrict__ par,
+                          int *__restrict__ nb) {
+    for (int j = s1 + blockIdx.x * blockDim.x + threadIdx.x; j < s1 + T; j += gridDim.x * blockDim.x) {
+        const int pe = nb[par[j]];
+        nb[j] = (j + 1 < s1 + T && na[j + 1] < pe) ? na[j + 1] : pe;
+    }
+}
+
+// node records of nodes [s, e), deepest level first: a leaf's box over its
+// centroids, an inner node's over its children's boxes (float min / max of
+// outward-rounded bounds are exact)
+__global__ void k_oct_box(int s, int e, const int *__restrict__ na, const int *__restrict__ nb,
+                          const int *__restrict__ first, const int *__restrict__ nch,
+                          const d4 *__restrict__ cs, float4 *__restrict__ onode) {
+    for (int j = s + blockIdx.x * blockDim.x + threadIdx.x; j < e; j += gridDim.x * blockDim.x) {
+        float4 lo, hi;
+        if (nch[j] == 0) {
+            double l[3] = {INFINITY, INFINITY, INFINITY}, h[3] = {-INFINITY, -INFINITY, -INFINITY};
+            for (int k = na[j]; k < nb[j]; k++) {
+                const d4 c = cs[k];
+                l[0] = fmin(l[0], c.x); l[1] = fmin(l[1], c.y); l[2] = fmin(l[2], c.z);
+                h[0] = fmax(h[0], c.x); h[1] = fmax(h[1], c.y); h[2] = fmax(h[2], c.z);
             }
-            if (f == 4) break;
-            const int nb = comp(M.tn[t], f);
-            if (nb < 0) break;  // centre outside the super-simplex: keep the last tet
-            t = nb;
-            if (step == (1 << 22) - 1) t = t0;  // no convergence: keep the parent's seed
+            lo = make_float4(__double2float_rd(l[0]), __double2float_rd(l[1]), __double2float_rd(l[2]),
+                             __int_as_float(na[j]));
+            hi = make_float4(__double2float_ru(h[0]), __double2float_ru(h[1]), __double2float_ru(h[2]),
+                             __int_as_float(-(nb[j] - na[j])));
+        } else {
+            lo = make_float4(INFINITY, INFINITY, INFINITY, __int_as_float(first[j]));
+            hi = make_float4(-INFINITY, -INFINITY, -INFINITY, __int_as_float(nch[j]));
+            for (int c = first[j]; c < first[j] + nch[j]; c++) {
+                const float4 a = onode[2 * c], b = onode[2 * c + 1];
+                lo.x = fminf(lo.x, a.x); lo.y = fminf(lo.y, a.y); lo.z = fminf(lo.z, a.z);
+                hi.x = fmaxf(hi.x, b.x); hi.y = fmaxf(hi.y, b.y); hi.z = fmaxf(hi.z, b.z);
+            }
         }
-        out[c] = t;
+        onode[2 * j] = lo;
+        onode[2 * j + 1] = hi;
     }
 }
 
@@ -268,14 +362,6 @@ struct Centroid {
     double c[3];
 };
 
-__device__ __forceinline__ unsigned spread3(unsigned v) {  // 10 bits -> every third bit
-    v &= 0x3ffu;
-    v = (v | (v << 16)) & 0x030000ffu;
-    v = (v | (v << 8)) & 0x0300f00fu;
-    v = (v | (v << 4)) & 0x030c30c3u;
-    v = (v | (v << 2)) & 0x09249249u;
-    return v;
-}
 
 template <class QT>
 __global__ void k_bucket(const QT *__restrict__ Q, int64_t M, Centroid cen, MeshView mv, int bits,
@@ -385,53 +471,73 @@ __global__ void k_scan_apply(const int *__restrict__ in, int64_t n, const OutT *
 // row sinks
 // ---------------------------------------------------------------------------
 
-// get_weights: rows staged per original row index, compacted afterwards
+// get_weights, count pass: every row's neighbour count and normaliser; rows
+// of at most ROW_STAGE entries are staged at i * ROW_STAGE, longer rows are
+// queued (refill) and recomputed straight into the final CSR by the fill
+// pass, as are the rows the large kernel handled (their queue is the large-
+// row list).  So no row ever needs more room than its final CSR slice.
 struct StageSink {
     static constexpr bool FULL = true;
-    int *__restrict__ cnt;          // [M]
-    int64_t *__restrict__ src;      // [M] first staged entry of the row
-    int *__restrict__ cols;         // [M*ROW_CAP + arena]
-    double *__restrict__ vals;      // [M*ROW_CAP + arena]
-    int64_t arena_base;             // = M*ROW_CAP
-    int64_t arena_cap;
+    int *__restrict__ cnt;          // [M] entries of the row (0 for empty / failed rows)
+    uint8_t *__restrict__ staged;   // [M] 1: the row is staged
+    int *__restrict__ cols;         // [M * ROW_STAGE]
+    double *__restrict__ vals;      // [M * ROW_STAGE]
+    int *__restrict__ refill;       // [M] fast-kernel rows longer than ROW_STAGE
     DevSummary *sum;
     double *__restrict__ total;     // [M] normaliser of each row (0 for empty rows)
 
     template <int G, class W>
     __device__ __forceinline__ void emit(int64_t i, int nnb, W &ws, const Grp<G> &g, bool large,
                                          const MeshView &, dv3, const RowInfo &r) {
-        if (g.lane == 0) total[i] = (nnb > 0) ? r.total : 0.0;
-        int64_t o = i * ROW_CAP;
-        if (large) {
-            unsigned long long a = 0;
-            if (g.lane == 0) a = atomicAdd(&sum->arena_used, (unsigned long long)nnb);
-            a = __shfl_sync(g.mask, a, 0, G);
-            if ((int64_t)(a + nnb) > arena_cap) {
-                if (g.lane == 0) {
-                    cnt[i] = 0;
-                    src[i] = 0;
-                    atomicAdd(&sum->rows_failed, 1ull);
-                    atomicCAS(&sum->first_status, 0, NIF_ERR_CAPACITY);
-                }
-                return;
+        const bool stage = !large && nnb <= ROW_STAGE;
+        if (stage) {
+            const int64_t o = i * ROW_STAGE;
+            for (int s = g.lane; s < nnb; s += G) {
+                cols[o + s] = ws.nbr_vid[s];
+                vals[o + s] = ws.acc[s];
             }
-            o = arena_base + (int64_t)a;
-        }
-        for (int s = g.lane; s < nnb; s += G) {
-            cols[o + s] = ws.nbr_vid[s];
-            vals[o + s] = ws.acc[s];
         }
         if (g.lane == 0) {
+            total[i] = (nnb > 0) ? r.total : 0.0;
             cnt[i] = nnb;
-            src[i] = o;
+            staged[i] = stage ? 1 : 0;
+            if (!large && !stage) refill[atomicAdd(&sum->refill_count, 1)] = (int)i;
         }
     }
     __device__ __forceinline__ void empty(int64_t i, int lane) {
         if (lane == 0) {
             cnt[i] = 0;
-            src[i] = 0;
+            staged[i] = 1;
+            total[i] = 0.0;
         }
     }
+};
+
+// get_weights, fill pass: a queued row recomputed into its final CSR slice
+// (the same routine as the count pass, hence the same entries); a row whose
+// count differs from its slice is an internal error and writes nothing
+template <class VT>
+struct DirectSink {
+    static constexpr bool FULL = true;
+    const int32_t *__restrict__ rowptr;
+    int32_t *__restrict__ cols;
+    VT *__restrict__ vals;
+    DevSummary *sum;
+
+    template <int G, class W>
+    __device__ __forceinline__ void emit(int64_t i, int nnb, W &ws, const Grp<G> &g, bool,
+                                         const MeshView &, dv3, const RowInfo &) {
+        const int64_t o = rowptr[i];
+        if (rowptr[i + 1] - o != nnb) {
+            if (g.lane == 0) atomicCAS(&sum->first_status, 0, NIF_ERR_INTERNAL);
+            return;
+        }
+        for (int s = g.lane; s < nnb; s += G) {
+            cols[o + s] = ws.nbr_vid[s];
+            vals[o + s] = (VT)ws.acc[s];
+        }
+    }
+    __device__ __forceinline__ void empty(int64_t, int) {}
 };
 
 template <class T> struct Arith;
@@ -772,10 +878,13 @@ __device__ __forceinline__ void record(DevSummary *sum, const RowInfo &r, int la
 template <class QT, class Sink, int PM, int OCC>
 __global__ void __launch_bounds__(FAST_BLOCK, OCC) k_rows_fast(MeshView M, const QT *__restrict__ Q,
                                                           Centroid cen, const int *__restrict__ order,
-                                                          int64_t nrows, Sink sink, LargeQueue lq,
+                                                          int64_t nrows, const int *nrows_dev,
+                                                          Sink sink, LargeQueue lq,
                                                           DevSummary *sum, int tile,
                                                           unsigned long long *counter) {
     extern __shared__ __align__(16) unsigned char smem[];
+    // a row count known only on the device (a queue's length) bounds nrows
+    if (nrows_dev) nrows = min(nrows, (int64_t)*nrows_dev);
     constexpr int G = FAST_G;
     constexpr int GPB = FAST_BLOCK / G;
     Grp<G> g;
@@ -862,21 +971,22 @@ __global__ void __launch_bounds__(32) k_rows_large(MeshView M, const QT *__restr
     if (g.lane == 0 && steps) atomicAdd(&sum->walk_steps, steps);
 }
 
-// CSR compaction: 16 lanes per row
+// CSR compaction of the staged rows: 8 lanes per row
 template <class VT>
-__global__ void k_compact(int64_t M, const int *__restrict__ cnt, const int64_t *__restrict__ src,
+__global__ void k_compact(int64_t M, const int *__restrict__ cnt, const uint8_t *__restrict__ staged,
                           const int *__restrict__ scols, const double *__restrict__ svals,
                           const int32_t *__restrict__ rowptr, int32_t *__restrict__ cols,
                           VT *__restrict__ vals) {
     const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t u = tid; u < M * 16; u += stride) {
-        const int64_t i = u >> 4;
-        const int l = (int)(u & 15);
+    for (int64_t u = tid; u < M * 8; u += stride) {
+        const int64_t i = u >> 3;
+        if (!staged[i]) continue;
+        const int l = (int)(u & 7);
         const int n = cnt[i];
-        const int64_t s = src[i];
+        const int64_t s = i * ROW_STAGE;
         const int64_t d = rowptr[i];
-        for (int k = l; k < n; k += 16) {
+        for (int k = l; k < n; k += 8) {
             cols[d + k] = scols[s + k];
             vals[d + k] = (VT)svals[s + k];
         }
@@ -920,6 +1030,7 @@ struct nif_dmesh {
     int num_sms;
     size_t bytes;
     int64_t orient_unc, orient_flip;  // tets with an uncertain / flipped orientation flag
+    int oct_nodes, oct_levels;        // centroid octree: nodes, node levels
     nif_tuning tune{OCC_DEFAULT, 0, MESH_TILE_DEFAULT, 0};
 };
 
@@ -950,23 +1061,56 @@ inline int cuda_rc(cudaError_t e) { return e == cudaSuccess ? NIF_OK : NIF_ERR_C
         if (e_ != cudaSuccess) return NIF_ERR_CUDA;     \
     } while (0)
 
-// Seed-grid cells per key (rounded up to a power of two, at most 2^26 cells).
-// A query's walk starts from the tet holding its cell's centre.  Where
-// natinterp3d's fast orientation signs make a query look inside two tets
-// (near-degenerate geometry), the tet its walk ends in -- and with it the
-// visiting order and the last bits of the weights -- depends on the seed.
-// One cell per key reproduces natinterp3d's results on every golden case;
-// 64 cells per key (1.54 instead of 3.27 walk steps, 5 % faster at 1M keys)
-// changes the last bits of some rows of the lattice + mixture golden.
-#ifndef NIF_GRID_CELLS_PER_KEY
-#define NIF_GRID_CELLS_PER_KEY 1
-#endif
-size_t grid_cells_max(int n_vertices) {
-    size_t n = n_vertices > 4 ? (size_t)(n_vertices - 4) : 1;
-    n *= NIF_GRID_CELLS_PER_KEY;
-    size_t c = 1;
-    while (c < n && c < ((size_t)1 << 26)) c <<= 1;
-    return c;
+// Octree nodes the resident mesh has room for.  A typical mesh needs far
+// fewer (about one per 50 tets on uniform keys); where a level would exceed
+// the room, its nodes stay leaves -- larger leaves, same results.
+int oct_node_cap(int nt) { return nt / 8 + 1024; }
+
+// Scratch of the centroid sort and octree build at mesh creation, carved
+// from the start of the face-circumcentre array (filled only afterwards).
+struct OctScratch {
+    uint32_t *chi, *clo, *key_a, *key_b;
+    int32_t *idx_a, *idx_b;
+    int *hist, *off, *bsum, *tot;
+    int64_t nblocks;
+    unsigned long long *code;
+    int *node_of, *flag, *scan;
+    int *na, *nb, *par, *first, *nch;
+};
+
+OctScratch carve_oct_scratch(Carve &c, int nt) {
+    OctScratch S;
+    const int cap = oct_node_cap(nt);
+    S.nblocks = (nt + RS_TILE - 1) / RS_TILE;
+    S.chi = c.take<uint32_t>(nt);
+    S.clo = c.take<uint32_t>(nt);
+    S.key_a = c.take<uint32_t>(nt);
+    S.key_b = c.take<uint32_t>(nt);
+    S.idx_a = c.take<int32_t>(nt);
+    S.idx_b = c.take<int32_t>(nt);
+    S.hist = c.take<int>(16 * S.nblocks);
+    S.off = c.take<int>(16 * S.nblocks);
+    S.bsum = c.take<int>((16 * S.nblocks + nt + SCAN_TILE - 1) / SCAN_TILE + 1);
+    S.tot = c.take<int>(2);
+    S.code = c.take<unsigned long long>(nt);
+    S.node_of = c.take<int>(nt);
+    S.flag = c.take<int>(nt);
+    S.scan = c.take<int>(nt);
+    S.na = c.take<int>(cap);
+    S.nb = c.take<int>(cap);
+    S.par = c.take<int>(cap);
+    S.first = c.take<int>(cap);
+    S.nch = c.take<int>(cap);
+    return S;
+}
+
+// face-circumcentre slots: 4 per tet, more for tiny meshes so that the
+// build scratch fits
+size_t fcc_slots(int nt) {
+    Carve c{nullptr, 0, (size_t)-1, true};
+    carve_oct_scratch(c, nt);
+    const size_t need = (align_up(c.off, 256) + sizeof(d4) - 1) / sizeof(d4);
+    return need > 4 * (size_t)nt ? need : 4 * (size_t)nt;
 }
 
 struct MeshLayout {
@@ -974,7 +1118,9 @@ struct MeshLayout {
     int4 *tv, *tn;
     uint32_t *tinfo;
     d4 *tcc, *fcc;
-    int *grid_a, *grid_b;  // ping-pong seed levels
+    d4 *cs;                      // sorted centroids
+    float4 *onode;               // octree node records, two float4 each
+    unsigned long long *omask;   // octree child digits
     double *bbox_part;
     int *flag;
 };
@@ -986,10 +1132,10 @@ MeshLayout carve_mesh(Carve &c, int nv, int nt) {
     L.tn = c.take<int4>(nt);
     L.tinfo = c.take<uint32_t>(nt);
     L.tcc = c.take<d4>(nt);
-    L.fcc = c.take<d4>(4 * (size_t)nt);
-    const size_t gm = grid_cells_max(nv);
-    L.grid_a = c.take<int>(gm);
-    L.grid_b = c.take<int>(gm);
+    L.fcc = c.take<d4>(fcc_slots(nt));
+    L.cs = c.take<d4>(nt);
+    L.onode = c.take<float4>(2 * (size_t)oct_node_cap(nt));
+    L.omask = c.take<unsigned long long>(oct_node_cap(nt));
     L.bbox_part = c.take<double>(6 * 256);
     L.flag = c.take<int>(4);
     return L;
@@ -1014,14 +1160,16 @@ struct QueryLayout {
     double *exact;          // NIF_EXACT_SCRATCH doubles per large-row group
     // weights mode only
     int *cnt;
-    int64_t *src, *off64;
-    int *scols;
+    uint8_t *staged;
+    int64_t *off64;
+    int *scols;             // staged rows, ROW_STAGE entries each
     double *svals;
     double *rtot;           // per-row normaliser
-    int64_t arena_cap;
+    int *refill;            // fast-kernel rows longer than ROW_STAGE
+    DevSummary *fill_sum;   // counters of the fill pass's recomputed rows
 };
 
-int bucket_bits(int64_t M) {
+constexpr int bucket_bits(int64_t M) {
     int b = 1;
     while (b < 10 && ((int64_t)1 << (3 * (b + 1))) <= M / 2) b++;
     return b;
@@ -1046,14 +1194,15 @@ QueryLayout carve_query(Carve &c, int64_t M, int mode) {
     L.large_ws = c.take<LargeWS>(LARGE_GROUPS);
     L.exact = c.take<double>((size_t)LARGE_GROUPS * NIF_EXACT_SCRATCH);
     if (mode == NIF_MODE_WEIGHTS) {
-        L.arena_cap = (int64_t)1 << 22;
-        const int64_t stage = M * ROW_CAP + L.arena_cap;
-        L.cnt = c.take<int>(M > 0 ? M : 1);
-        L.src = c.take<int64_t>(M > 0 ? M : 1);
+        const int64_t m1 = M > 0 ? M : 1;
+        L.cnt = c.take<int>(m1);
+        L.staged = c.take<uint8_t>(m1);
         L.off64 = c.take<int64_t>(M + 1);
-        L.scols = c.take<int>(stage);
-        L.svals = c.take<double>(stage);
-        L.rtot = c.take<double>(M > 0 ? M : 1);
+        L.scols = c.take<int>(m1 * ROW_STAGE);
+        L.svals = c.take<double>(m1 * ROW_STAGE);
+        L.rtot = c.take<double>(m1);
+        L.refill = c.take<int>(m1);
+        L.fill_sum = c.take<DevSummary>(1);
     }
     return L;
 }
@@ -1075,26 +1224,58 @@ int set_smem(Kern k, size_t bytes) {
     return cuda_rc(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
 }
 
+// Resident blocks per SM of kernel k with `smem` bytes of dynamic shared
+// memory, on the current device.  The first call per (kernel, device) sets
+// the kernel's shared-memory limit there and queries the occupancy; the
+// answer is cached, and concurrent first calls from several host threads are
+// serialised.
+template <class Kern>
+int resident_blocks(Kern k, int threads, size_t smem) {
+    constexpr int DEVS = 64;
+    static std::mutex mu;
+    static int cache[DEVS] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) dev = -1;
+    std::lock_guard<std::mutex> lock(mu);
+    if (dev >= 0 && dev < DEVS && cache[dev] > 0) return cache[dev];
+    if (smem > 48 * 1024) set_smem(k, smem);
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k, threads, smem) != cudaSuccess || n < 1)
+        n = 1;
+    if (dev >= 0 && dev < DEVS) cache[dev] = n;
+    return n;
+}
+
 // Optional phase timing (nif_profile_enable / nif_profile_read): events
-// recorded on the launching stream between the phases of a query call.
+// recorded on the launching stream between the phases of a query call, one
+// set per call in a ring of PROF_RING sets, so that timed loops never wait
+// on the host; nif_profile_read averages the calls recorded since the last
+// enable or read.
 constexpr int PROF_EVENTS = 5;  // start | bucketing | fast rows | large rows | finish
+constexpr int PROF_RING = 64;
 struct Profiler {
     bool on = false;
     bool created = false;
-    int recorded = 0;
-    cudaEvent_t ev[PROF_EVENTS];
+    int calls = 0;     // calls started since enable / read (the ring keeps the last PROF_RING)
+    int marks = 0;     // marks of the current call
+    cudaEvent_t ev[PROF_RING][PROF_EVENTS];
 };
 Profiler g_prof;
 
 inline void prof_mark(int k, cudaStream_t st) {
     if (!g_prof.on) return;
     if (!g_prof.created) {
-        for (int i = 0; i < PROF_EVENTS; i++) cudaEventCreate(&g_prof.ev[i]);
+        for (int r = 0; r < PROF_RING; r++)
+            for (int i = 0; i < PROF_EVENTS; i++) cudaEventCreate(&g_prof.ev[r][i]);
         g_prof.created = true;
     }
-    cudaEventRecord(g_prof.ev[k], st);
-    if (k + 1 > g_prof.recorded) g_prof.recorded = k + 1;
-    if (k == 0) g_prof.recorded = 1;
+    if (k == 0) {
+        g_prof.calls++;
+        g_prof.marks = 0;
+    }
+    if (g_prof.calls == 0) return;
+    cudaEventRecord(g_prof.ev[(g_prof.calls - 1) % PROF_RING][k], st);
+    g_prof.marks = k + 1;
 }
 
 // bucket the queries (writes L.order); positions fit int32 because M < 2^31
@@ -1113,20 +1294,29 @@ void run_bucketing(const nif_dmesh *m, const QT *Q, int64_t M, const Centroid &c
     prof_mark(1, st);
 }
 
+// The rows a fast-kernel launch takes: positions [0, nrows) of `order`
+// (nrows further bounded by *nrows_dev when that is set), rows it cannot hold
+// queued in `large`, counters in `sum`.
+struct RowSet {
+    const int *order;
+    const int *nrows_dev;
+    int *large;
+    DevSummary *sum;
+    unsigned long long *counter;
+};
+
+inline RowSet all_rows(const QueryLayout &L) {
+    return RowSet{L.order, nullptr, L.large_list, L.sum, L.counter};
+}
+
 // persistent grid of the fast row kernel: resident blocks per SM x SMs
 template <class QT, class Sink, int PM, int OCC>
 void launch_fast_occ(const nif_dmesh *m, const QT *Q, int64_t M, const Centroid &cen,
-                     const QueryLayout &L, const Sink &sink, cudaStream_t st) {
+                     const RowSet &R, const Sink &sink, cudaStream_t st) {
     constexpr int GPB = FAST_BLOCK / FAST_G;
     const size_t smem = GPB * sizeof(FastWS);
     auto kern = k_rows_fast<QT, Sink, PM, OCC>;
-    static int per_sm = -1;  // resident blocks per SM of this instantiation
-    if (per_sm < 0) {
-        if (smem > 48 * 1024) set_smem(kern, smem);
-        per_sm = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, FAST_BLOCK, smem);
-        if (per_sm < 1) per_sm = 1;
-    }
+    const int per_sm = resident_blocks(kern, FAST_BLOCK, smem);
     // tile is an upper bound: a call too small to give every resident group
     // two tiles takes smaller ones (or the static stride), so that small
     // calls keep the whole GPU busy
@@ -1140,22 +1330,22 @@ void launch_fast_occ(const nif_dmesh *m, const QT *Q, int64_t M, const Centroid 
     const int64_t cap = (int64_t)per_sm * m->num_sms;
     if (blocks > cap) blocks = cap;
     if (blocks < 1) blocks = 1;
-    if (tile > 0) cudaMemsetAsync(L.counter, 0, sizeof(unsigned long long), st);
-    kern<<<(unsigned)blocks, FAST_BLOCK, smem, st>>>(m->view, Q, cen, L.order, M, sink,
-                                                    LargeQueue{L.large_list}, L.sum, tile, L.counter);
+    if (tile > 0) cudaMemsetAsync(R.counter, 0, sizeof(unsigned long long), st);
+    kern<<<(unsigned)blocks, FAST_BLOCK, smem, st>>>(m->view, Q, cen, R.order, M, R.nrows_dev, sink,
+                                                    LargeQueue{R.large}, R.sum, tile, R.counter);
 }
 
 // the structure-only (gradient) rows keep their own occupancy; the others
 // run at the mesh's tuned one
 template <class QT, class Sink, int PM>
 void launch_fast(const nif_dmesh *m, const QT *Q, int64_t M, const Centroid &cen,
-                 const QueryLayout &L, const Sink &sink, cudaStream_t st) {
+                 const RowSet &R, const Sink &sink, cudaStream_t st) {
     if constexpr (!Sink::FULL)
-        launch_fast_occ<QT, Sink, PM, Sink::MIN_BLOCKS>(m, Q, M, cen, L, sink, st);
+        launch_fast_occ<QT, Sink, PM, Sink::MIN_BLOCKS>(m, Q, M, cen, R, sink, st);
     else if (m->tune.blocks_per_sm == OCC_LO)
-        launch_fast_occ<QT, Sink, PM, OCC_LO>(m, Q, M, cen, L, sink, st);
+        launch_fast_occ<QT, Sink, PM, OCC_LO>(m, Q, M, cen, R, sink, st);
     else
-        launch_fast_occ<QT, Sink, PM, OCC_HI>(m, Q, M, cen, L, sink, st);
+        launch_fast_occ<QT, Sink, PM, OCC_HI>(m, Q, M, cen, R, sink, st);
 }
 
 // fast rows (filtered when the mesh's predicate mode is not the default),
@@ -1164,13 +1354,29 @@ template <class QT, class Sink>
 void run_rows(const nif_dmesh *m, const QT *Q, int64_t M, const Centroid &cen, const QueryLayout &L,
               const Sink &sink, cudaStream_t st, int large_groups = LARGE_GROUPS) {
     if (m->view.pmode == PRED_FAST)
-        launch_fast<QT, Sink, PM_PLAIN>(m, Q, M, cen, L, sink, st);
+        launch_fast<QT, Sink, PM_PLAIN>(m, Q, M, cen, all_rows(L), sink, st);
     else
-        launch_fast<QT, Sink, PM_FILTER>(m, Q, M, cen, L, sink, st);
+        launch_fast<QT, Sink, PM_FILTER>(m, Q, M, cen, all_rows(L), sink, st);
     prof_mark(2, st);
     k_rows_large<QT, Sink><<<large_groups, 32, 0, st>>>(m->view, Q, cen, LargeQueue{L.large_list},
                                                         sink, L.large_ws, L.exact, L.sum);
     prof_mark(3, st);
+}
+
+// fill pass of get_weights: the count pass's queued rows again, into the CSR
+template <class QT, class Sink>
+void refill_rows(const nif_dmesh *m, const QT *Q, int64_t M, const Centroid &cen, const QueryLayout &L,
+                 const Sink &sink, cudaStream_t st) {
+    // fast-kernel rows longer than ROW_STAGE: the queue's length is on the device
+    const RowSet R{L.refill, &L.sum->refill_count, L.large_list, L.fill_sum, L.counter};
+    if (m->view.pmode == PRED_FAST)
+        launch_fast<QT, Sink, PM_PLAIN>(m, Q, M, cen, R, sink, st);
+    else
+        launch_fast<QT, Sink, PM_FILTER>(m, Q, M, cen, R, sink, st);
+    // the rows the large kernel handled (their queue is intact: refilled rows
+    // all fit the fast kernel, so nothing is appended to it)
+    k_rows_large<QT, Sink><<<LARGE_GROUPS, 32, 0, st>>>(m->view, Q, cen, LargeQueue{L.large_list},
+                                                        sink, L.large_ws, L.exact, L.fill_sum);
 }
 
 __global__ void k_rowptr_guarded(const int64_t *__restrict__ off, int64_t M,
@@ -1269,19 +1475,139 @@ NIF_EXPORT int nif_dmesh_create(const double *d_vxyz, const int32_t *d_tet_v,
     V.nt = n_tets;
     V.pmode = PRED_FAST;
 
+    V.cs = L.cs;
+    V.onode = L.onode;
+    V.omask = L.omask;
+
     int rc = NIF_OK;
     do {
         if (cudaMemsetAsync(L.flag, 0, 4 * sizeof(int), st) != cudaSuccess) { rc = NIF_ERR_CUDA; break; }
         k_prep_vertices<<<blocks_for(n_vertices, 256), 256, 0, st>>>(d_vxyz, n_vertices, L.vtx);
         k_prep_tets<<<blocks_for(n_tets, 256), 256, 0, st>>>(d_tet_v, d_tet_n, n_vertices, n_tets,
                                                              L.tv, L.tn, L.flag);
-        k_prep_geometry<<<blocks_for(n_tets, 128), 128, 0, st>>>(V, L.tinfo, L.tcc, L.fcc, L.flag);
         const int nbb = blocks_for(V.n, 256, 256);
         k_bbox_partial<<<nbb, 256, 0, st>>>(L.vtx, V.n, L.bbox_part);
         double part[6 * 256];
-        int flag[4];
         if (cudaMemcpyAsync(part, L.bbox_part, sizeof(double) * 6 * nbb, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
-            cudaMemcpyAsync(flag, L.flag, sizeof(flag), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+            cudaStreamSynchronize(st) != cudaSuccess) {
+            rc = NIF_ERR_CUDA;
+            break;
+        }
+        double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+        for (int b = 0; b < nbb; b++)
+            for (int a = 0; a < 3; a++) {
+                lo[a] = fmin(lo[a], part[6 * b + a]);
+                hi[a] = fmax(hi[a], part[6 * b + 3 + a]);
+            }
+        double ext[3], emax = 0.0;
+        for (int a = 0; a < 3; a++) {
+            ext[a] = hi[a] - lo[a];
+            if (!(ext[a] > 0.0) || !isfinite(ext[a])) ext[a] = 0.0;
+            emax = fmax(emax, ext[a]);
+        }
+        if (!(emax > 0.0)) emax = 1.0;
+        for (int a = 0; a < 3; a++)
+            if (ext[a] < emax * 1e-3) ext[a] = emax * 1e-3;
+
+        // query bucketing normalises by the data bounding box
+        for (int a = 0; a < 3; a++) {
+            V.gdim[a] = 1;
+            V.glo[a] = lo[a];
+            V.ginv[a] = 1.0 / ext[a];
+        }
+        // centroid code space: the bounding box of all vertices (the
+        // super-simplex's four included), which holds every tet centroid
+        {
+            d4 sv[4];
+            if (cudaMemcpyAsync(sv, L.vtx + V.n, sizeof(sv), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+                cudaStreamSynchronize(st) != cudaSuccess) {
+                rc = NIF_ERR_CUDA;
+                break;
+            }
+            double olo[3] = {lo[0], lo[1], lo[2]}, ohi[3] = {hi[0], hi[1], hi[2]};
+            for (int k = 0; k < 4; k++) {
+                const double c[3] = {sv[k].x, sv[k].y, sv[k].z};
+                for (int a = 0; a < 3; a++) {
+                    olo[a] = fmin(olo[a], c[a]);
+                    ohi[a] = fmax(ohi[a], c[a]);
+                }
+            }
+            V.oext = 0.0;
+            for (int a = 0; a < 3; a++) {
+                double e = ohi[a] - olo[a];
+                if (!(e > 0.0) || !isfinite(e)) e = 1.0;
+                V.olo[a] = olo[a];
+                V.osc[a] = (double)(1 << OCT_BITS) / e;
+                V.oext = fmax(V.oext, e);
+            }
+        }
+        // centroid octree: centroids sorted by code (two 32-bit radix sorts,
+        // low word then high word), then node levels top down, then boxes
+        // bottom up.  The scratch is the face-circumcentre array.
+        {
+            Carve tc{reinterpret_cast<unsigned char *>(L.fcc), 0, sizeof(d4) * fcc_slots(n_tets), true};
+            const OctScratch T = carve_oct_scratch(tc, n_tets);
+            if (!tc.ok) { rc = NIF_ERR_INTERNAL; break; }
+            const int nb = blocks_for(n_tets, 256);
+            k_cen_code<<<nb, 256, 0, st>>>(V, T.chi, T.clo, T.key_a, T.idx_a);
+            uint32_t *kin = T.key_a, *kout = T.key_b;
+            int32_t *vin = T.idx_a, *vout = T.idx_b;
+            for (int word = 0; word < 2; word++) {
+                if (word == 1) k_gather_key<<<nb, 256, 0, st>>>(T.chi, vin, n_tets, kin);
+                for (int pass = 0; pass < 8; pass++) {
+                    k_rs_hist<<<(unsigned)T.nblocks, RS_THREADS, 0, st>>>(kin, n_tets, 4 * pass,
+                                                                           (int)T.nblocks, T.hist);
+                    launch_scan<int>(T.hist, 16 * T.nblocks, T.bsum, T.tot, T.off, st);
+                    k_rs_scatter<<<(unsigned)T.nblocks, RS_THREADS, 0, st>>>(
+                        kin, vin, n_tets, 4 * pass, (int)T.nblocks, T.off, kout, vout);
+                    std::swap(kin, kout);
+                    std::swap(vin, vout);
+                }
+            }
+            k_cen_gather<<<nb, 256, 0, st>>>(V, vin, T.chi, T.clo, L.cs, T.code);
+            const int cap = oct_node_cap(n_tets);
+            if (cudaMemsetAsync(T.node_of, 0, sizeof(int) * n_tets, st) != cudaSuccess ||
+                cudaMemsetAsync(T.nch, 0, sizeof(int) * cap, st) != cudaSuccess ||
+                cudaMemsetAsync(T.first, 0, sizeof(int) * cap, st) != cudaSuccess ||
+                cudaMemsetAsync(L.omask, 0, sizeof(unsigned long long) * cap, st) != cudaSuccess) {
+                rc = NIF_ERR_CUDA;
+                break;
+            }
+            const int root[2] = {0, n_tets};
+            if (cudaMemcpyAsync(T.na, &root[0], sizeof(int), cudaMemcpyHostToDevice, st) != cudaSuccess ||
+                cudaMemcpyAsync(T.nb, &root[1], sizeof(int), cudaMemcpyHostToDevice, st) != cudaSuccess) {
+                rc = NIF_ERR_CUDA;
+                break;
+            }
+            int lvl[OCT_KMAX + 2] = {0, 1};
+            int levels = 1;  // node levels built: [lvl[l], lvl[l + 1]) for l < levels
+            for (int k = 0; k < OCT_KMAX; k++) {
+                const int s0 = lvl[k], s1 = lvl[k + 1];
+                k_oct_flag<<<nb, 256, 0, st>>>(T.code, n_tets, T.node_of, T.na, T.nb, s0, s1, k, T.flag);
+                launch_scan<int>(T.flag, n_tets, T.bsum, T.tot, T.scan, st);
+                int tot = 0;
+                if (cudaMemcpyAsync(&tot, T.tot, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+                    cudaStreamSynchronize(st) != cudaSuccess) {
+                    rc = NIF_ERR_CUDA;
+                    break;
+                }
+                if (tot == 0 || (int64_t)s1 + tot > cap) break;  // no split / no room: leaves stay
+                k_oct_link<<<nb, 256, 0, st>>>(T.code, n_tets, T.node_of, T.na, T.nb, s0, s1, k, T.flag,
+                                               T.scan, T.par, T.first, T.nch, L.omask);
+                k_oct_end<<<blocks_for(tot, 256), 256, 0, st>>>(s1, tot, T.na, T.par, T.nb);
+                lvl[k + 2] = s1 + tot;
+                levels = k + 2;
+            }
+            if (rc != NIF_OK) break;
+            for (int l = levels - 1; l >= 0; l--)
+                k_oct_box<<<blocks_for(lvl[l + 1] - lvl[l], 128), 128, 0, st>>>(
+                    lvl[l], lvl[l + 1], T.na, T.nb, T.first, T.nch, L.cs, L.onode);
+            h->oct_nodes = lvl[levels];
+            h->oct_levels = levels;
+        }
+        k_prep_geometry<<<blocks_for(n_tets, 128), 128, 0, st>>>(V, L.tinfo, L.tcc, L.fcc, L.flag);
+        int flag[4];
+        if (cudaMemcpyAsync(flag, L.flag, sizeof(flag), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
             cudaStreamSynchronize(st) != cudaSuccess) {
             rc = NIF_ERR_CUDA;
             break;
@@ -1298,65 +1624,6 @@ NIF_EXPORT int nif_dmesh_create(const double *d_vxyz, const int32_t *d_tet_v,
             }
         }
         h->orient_flip = flag[2];
-        double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
-        for (int b = 0; b < nbb; b++)
-            for (int a = 0; a < 3; a++) {
-                lo[a] = fmin(lo[a], part[6 * b + a]);
-                hi[a] = fmax(hi[a], part[6 * b + 3 + a]);
-            }
-        // seed-grid resolution: about NIF_GRID_CELLS_PER_KEY cells per key,
-        // power-of-two per axis
-        double ext[3], emax = 0.0;
-        for (int a = 0; a < 3; a++) {
-            ext[a] = hi[a] - lo[a];
-            if (!(ext[a] > 0.0) || !isfinite(ext[a])) ext[a] = 0.0;
-            emax = fmax(emax, ext[a]);
-        }
-        if (!(emax > 0.0)) emax = 1.0;
-        double vol = 1.0;
-        for (int a = 0; a < 3; a++) {
-            if (ext[a] < emax * 1e-3) ext[a] = emax * 1e-3;
-            vol *= ext[a];
-        }
-        const size_t cmax = grid_cells_max(n_vertices);
-        const double side = cbrt(vol / (double)cmax);
-        int R[3], lv[3];
-        for (int a = 0; a < 3; a++) {
-            double r = ext[a] / side;
-            int l = 0;
-            while (l < 10 && (double)(1 << (l + 1)) <= r * 1.4142) l++;
-            lv[a] = l;
-        }
-        while (((size_t)1 << (lv[0] + lv[1] + lv[2])) > cmax) {
-            int a = (lv[0] >= lv[1] && lv[0] >= lv[2]) ? 0 : (lv[1] >= lv[2] ? 1 : 2);
-            lv[a]--;
-        }
-        for (int a = 0; a < 3; a++) {
-            R[a] = 1 << lv[a];
-            V.gdim[a] = R[a];
-            V.glo[a] = lo[a];
-            V.ginv[a] = (double)R[a] / ext[a];
-        }
-        const int levels = lv[0] > lv[1] ? (lv[0] > lv[2] ? lv[0] : lv[2]) : (lv[1] > lv[2] ? lv[1] : lv[2]);
-        int *cur = L.grid_a, *prev = nullptr;
-        int pd[3] = {1, 1, 1};
-        for (int k = 0; k <= levels; k++) {
-            int d[3];
-            for (int a = 0; a < 3; a++) d[a] = (1 << k) < R[a] ? (1 << k) : R[a];
-            const int nc = d[0] * d[1] * d[2];
-            k_seed_level<<<blocks_for(nc, 128), 128, 0, st>>>(V, d[0], d[1], d[2], pd[0], pd[1], pd[2],
-                                                              prev, cur, L.flag);
-            prev = cur;
-            cur = (cur == L.grid_a) ? L.grid_b : L.grid_a;
-            for (int a = 0; a < 3; a++) pd[a] = d[a];
-        }
-        V.grid = prev;
-        if (cudaMemcpyAsync(flag, L.flag, sizeof(flag), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
-            cudaStreamSynchronize(st) != cudaSuccess) {
-            rc = NIF_ERR_CUDA;
-            break;
-        }
-        if (flag[0]) rc = NIF_ERR_INTERNAL;
         if (cudaGetLastError() != cudaSuccess) rc = NIF_ERR_CUDA;
     } while (0);
     if (rc != NIF_OK) {
@@ -1373,9 +1640,9 @@ NIF_EXPORT int nif_dmesh_info(const nif_dmesh *m, int64_t info[8]) {
     if (!m || !info) return NIF_ERR_ARG;
     info[0] = m->n_vertices;
     info[1] = m->n_tets;
-    info[2] = m->view.gdim[0];
-    info[3] = m->view.gdim[1];
-    info[4] = m->view.gdim[2];
+    info[2] = m->oct_nodes;
+    info[3] = m->oct_levels;
+    info[4] = 0;
     info[5] = m->orient_unc;
     info[6] = m->orient_flip;
     info[7] = m->view.pmode;
@@ -1434,7 +1701,7 @@ NIF_EXPORT int nif_weights_count(const nif_dmesh *m, const void *d_queries, int 
     Centroid cen{{centroid[0], centroid[1], centroid[2]}};
     NIF_CUDA(cudaMemsetAsync(L.sum, 0, sizeof(DevSummary), st));
     if (M > 0) {
-        StageSink sink{L.cnt, L.src, L.scols, L.svals, M * ROW_CAP, L.arena_cap, L.sum, L.rtot};
+        StageSink sink{L.cnt, L.staged, L.scols, L.svals, L.refill, L.sum, L.rtot};
         if (query_dtype == NIF_F64) {
             run_bucketing(m, static_cast<const double *>(d_queries), M, cen, L, st);
             run_rows(m, static_cast<const double *>(d_queries), M, cen, L, sink, st);
@@ -1454,10 +1721,34 @@ NIF_EXPORT int nif_weights_count(const nif_dmesh *m, const void *d_queries, int 
     return NIF_OK;
 }
 
-NIF_EXPORT int nif_weights_fill(const nif_dmesh *m, int64_t M, const void *d_ws, size_t ws_bytes,
+namespace {
+// the fill pass: staged rows copied into the CSR, then the queued rows
+// (longer than ROW_STAGE, or handled by the large kernel) recomputed into
+// their slices from the same queries
+template <class VT>
+int fill_typed(const nif_dmesh *m, const void *q, int qdt, int64_t M, const Centroid &cen,
+               const QueryLayout &L, const int32_t *rowptr, VT *vals, int32_t *cols, cudaStream_t st) {
+    k_compact<VT><<<blocks_for(M * 8, 256), 256, 0, st>>>(M, L.cnt, L.staged, L.scols, L.svals, rowptr,
+                                                         cols, vals);
+    // the refill passes count into their own record; the large kernel reads
+    // its queue length from there
+    NIF_CUDA(cudaMemcpyAsync(L.fill_sum, L.sum, sizeof(DevSummary), cudaMemcpyDeviceToDevice, st));
+    DirectSink<VT> sink{rowptr, cols, vals, L.fill_sum};
+    if (qdt == NIF_F64)
+        refill_rows(m, static_cast<const double *>(q), M, cen, L, sink, st);
+    else
+        refill_rows(m, static_cast<const float *>(q), M, cen, L, sink, st);
+    return cuda_rc(cudaGetLastError());
+}
+}  // namespace
+
+NIF_EXPORT int nif_weights_fill(const nif_dmesh *m, const void *d_queries, int query_dtype, int64_t M,
+                                const double centroid[3], const void *d_ws, size_t ws_bytes,
                                 const int32_t *d_rowptr, void *d_vals, int vals_dtype,
                                 int32_t *d_cols, double *d_row_totals, void *stream) {
-    if (!m || M < 0 || M > (int64_t)INT32_MAX || !d_ws || !d_rowptr) return NIF_ERR_ARG;
+    int rc = check_query_args(m, d_queries, query_dtype, M, centroid, d_ws);
+    if (rc != NIF_OK) return rc;
+    if (!d_rowptr) return NIF_ERR_ARG;
     if (vals_dtype != NIF_F64 && vals_dtype != NIF_F32) return NIF_ERR_ARG;
     size_t need = 0;
     nif_query_workspace_bytes(m, M, NIF_MODE_WEIGHTS, &need);
@@ -1467,16 +1758,14 @@ NIF_EXPORT int nif_weights_fill(const nif_dmesh *m, int64_t M, const void *d_ws,
     cudaStream_t st = S(stream);
     Carve c{reinterpret_cast<unsigned char *>(const_cast<void *>(d_ws)), 0, ws_bytes, true};
     QueryLayout L = carve_query(c, M, NIF_MODE_WEIGHTS);
-    const int blocks = blocks_for(M * 16, 256);
+    Centroid cen{{centroid[0], centroid[1], centroid[2]}};
     if (d_row_totals)
         NIF_CUDA(cudaMemcpyAsync(d_row_totals, L.rtot, sizeof(double) * M, cudaMemcpyDeviceToDevice, st));
     if (vals_dtype == NIF_F64)
-        k_compact<double><<<blocks, 256, 0, st>>>(M, L.cnt, L.src, L.scols, L.svals, d_rowptr, d_cols,
-                                                  static_cast<double *>(d_vals));
-    else
-        k_compact<float><<<blocks, 256, 0, st>>>(M, L.cnt, L.src, L.scols, L.svals, d_rowptr, d_cols,
-                                                 static_cast<float *>(d_vals));
-    return cuda_rc(cudaGetLastError());
+        return fill_typed<double>(m, d_queries, query_dtype, M, cen, L, d_rowptr,
+                                  static_cast<double *>(d_vals), d_cols, st);
+    return fill_typed<float>(m, d_queries, query_dtype, M, cen, L, d_rowptr,
+                             static_cast<float *>(d_vals), d_cols, st);
 }
 
 namespace {
@@ -1527,20 +1816,28 @@ NIF_EXPORT int nif_interpolate(const nif_dmesh *m, const void *d_queries, int qu
 
 NIF_EXPORT int nif_profile_enable(int on) {
     g_prof.on = on != 0;
-    g_prof.recorded = 0;
+    g_prof.calls = 0;
+    g_prof.marks = 0;
     return NIF_OK;
 }
 
 NIF_EXPORT int nif_profile_read(double ms[4]) {
     if (!ms) return NIF_ERR_ARG;
     for (int i = 0; i < 4; i++) ms[i] = 0.0;
-    if (!g_prof.created || g_prof.recorded < PROF_EVENTS) return NIF_ERR_ARG;
-    NIF_CUDA(cudaEventSynchronize(g_prof.ev[PROF_EVENTS - 1]));
-    for (int i = 0; i < 4; i++) {
-        float t = 0.f;
-        NIF_CUDA(cudaEventElapsedTime(&t, g_prof.ev[i], g_prof.ev[i + 1]));
-        ms[i] = t;
-    }
+    // complete calls in the ring: all but the current one if it is unfinished
+    const int last = g_prof.marks == PROF_EVENTS ? g_prof.calls : g_prof.calls - 1;
+    const int first = last - PROF_RING + 1 > 1 ? last - PROF_RING + 1 : 1;
+    if (!g_prof.created || last < 1) return NIF_ERR_ARG;
+    NIF_CUDA(cudaEventSynchronize(g_prof.ev[(last - 1) % PROF_RING][PROF_EVENTS - 1]));
+    for (int c = first; c <= last; c++)
+        for (int i = 0; i < 4; i++) {
+            float t = 0.f;
+            NIF_CUDA(cudaEventElapsedTime(&t, g_prof.ev[(c - 1) % PROF_RING][i],
+                                          g_prof.ev[(c - 1) % PROF_RING][i + 1]));
+            ms[i] += t / (last - first + 1);
+        }
+    g_prof.calls = 0;
+    g_prof.marks = 0;
     return NIF_OK;
 }
 
@@ -1612,6 +1909,31 @@ int noalloc_scratch(int dev, void **out) {
     *out = g_noalloc_addr[dev];
     return NIF_OK;
 }
+
+// Bytes carve_noalloc takes for M queries (the same takes, each 256-byte
+// aligned), so that the fixed array is checked against the largest call at
+// compile time.
+constexpr size_t noalloc_bytes(int64_t M) {
+    const int bits = bucket_bits(M);
+    const int64_t nbk = (int64_t)1 << (3 * bits);
+    const int64_t mscan = M > nbk ? M : nbk;
+    const int64_t m1 = M > 0 ? M : 1;
+    const size_t takes[] = {sizeof(DevSummary),
+                            sizeof(unsigned long long),
+                            sizeof(int) * (size_t)m1,
+                            sizeof(int) * (size_t)(nbk + 1),
+                            sizeof(int) * (size_t)m1,
+                            sizeof(int) * (size_t)m1,
+                            sizeof(int64_t) * (size_t)((mscan + SCAN_TILE - 1) / SCAN_TILE + 1),
+                            sizeof(int64_t),
+                            sizeof(LargeWS) * (size_t)NOALLOC_LARGE_GROUPS,
+                            sizeof(double) * (size_t)NOALLOC_LARGE_GROUPS * NIF_EXACT_SCRATCH};
+    size_t off = 0;
+    for (size_t t : takes) off = (off + 255) / 256 * 256 + t;
+    return off;
+}
+static_assert(noalloc_bytes(NIF_NOALLOC_MAX_QUERIES) <= NIF_NOALLOC_SCRATCH_BYTES,
+              "the fixed scratch array must hold the largest call nif_interpolate_noalloc accepts");
 
 // interpolate-mode layout with NOALLOC_LARGE_GROUPS large-row workspaces
 QueryLayout carve_noalloc(Carve &c, int64_t M) {
@@ -2086,13 +2408,7 @@ void launch_batch_rows_occ(const nif_dbatch *b, const QT *Q, int64_t M, const in
     constexpr int GPB = FAST_BLOCK / FAST_G;
     const size_t smem = GPB * sizeof(FastWS);
     auto kern = k_rows_batch<QT, Sink, PM, OCC>;
-    static int per_sm = -1;
-    if (per_sm < 0) {
-        if (smem > 40 * 1024) set_smem(kern, smem);
-        per_sm = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, FAST_BLOCK, smem);
-        if (per_sm < 1) per_sm = 1;
-    }
+    const int per_sm = resident_blocks(kern, FAST_BLOCK, smem);
     const int tile = b->tune.tile;
     const int64_t want = (M + (int64_t)GPB * tile - 1) / ((int64_t)GPB * tile);
     int64_t blocks = (int64_t)per_sm * b->num_sms;

@@ -2,8 +2,11 @@
 // lanes per query.
 //
 // Per query (natinterp3d's getWeightsSingleQueryIF, natural_insertionfree.c:591-738):
-//   1. locate   seed tet from a uniform grid, then natinterp3d's visibility walk
-//               (delaunay.c:398-405); the four face tests of a step run on 4 lanes
+//   1. locate   seed tet = the tet whose centroid is nearest to the query, as
+//               natinterp3d's k-d tree returns it (delaunay.c:392-395), found in
+//               an octree over the Morton-sorted centroids; then
+//               natinterp3d's visibility walk (delaunay.c:398-405), the four
+//               face tests of a step on 4 lanes
 //   2. cavity   the connected set of tets whose circumsphere strictly contains
 //               the query (inspherefast > 0, natural_insertionfree.c:502-530),
 //               found breadth-first with all lanes testing in parallel; a
@@ -44,7 +47,6 @@ namespace nif {
 constexpr int ST_OK = 0;
 constexpr int ST_WALK = 1;       // walk step limit
 constexpr int ST_CAPACITY = 2;   // per-query capacity of this kernel exceeded
-constexpr int ST_ARENA = 3;      // large-row output arena full
 constexpr int ST_UNCERTAIN = 4;  // a predicate needs exact evaluation (PM_FILTER only)
 
 // predicate modes of a mesh (MeshView::pmode)
@@ -58,12 +60,16 @@ constexpr int PM_FILTER = 1;
 constexpr int PM_RESOLVE = 2;
 
 constexpr int WALK_LIMIT = 1 << 16;
+constexpr int SEED_STEP_LIMIT = 1 << 16;  // node and leaf visits of one nearest-centroid search
+constexpr int OCT_BITS = 20;              // centroid code: cell bits per axis
+constexpr int OCT_KMAX = 10;              // octree node levels below the root (6 code bits each)
+constexpr int OCT_SPLIT = 128;            // a node with more centroids than this has children
 
 struct __align__(32) d4 {
     double x, y, z, w;
 };
 
-// Resident mesh (device pointers) + seed grid parameters, passed by value.
+// Resident mesh (device pointers) and its parameters, passed by value.
 struct MeshView {
     const d4 *__restrict__ vtx;        // [nv] x, y, z, 0
     const int4 *__restrict__ tv;       // [nt] vertex ids
@@ -73,12 +79,26 @@ struct MeshView {
                                        // bits 8+2j: mirror slot of face j
     const d4 *__restrict__ tcc;        // [nt] tet circumcentre
     const d4 *__restrict__ fcc;        // [nt*4] circumcentre of the face opposite p[i]
-    const int *__restrict__ grid;      // seed tets of the finest grid level
+    // Tet centroids, (p0 + p1 + p2 + p3) / 4 per axis as natinterp3d's
+    // constructor computes them for its k-d tree (delaunay.c:151-157), sorted
+    // by a 60-bit Morton code of their cell in a 2^20 grid per axis over the
+    // bounding box of all vertices: x, y, z and the tet id (as a double).
+    // An octree over that order: node k spans the centroids of one octree
+    // cell, two octree levels (64 sub-cells, one 6-bit code digit) per node
+    // level.  onode[2 k] = float box lo (w: first child node, or first
+    // centroid of a leaf, as int bits); onode[2 k + 1] = box hi (w: number of
+    // children, or minus the centroid count of a leaf); omask[k] = the
+    // digits of the children present.  Boxes are rounded outwards.
+    const d4 *__restrict__ cs;
+    const float4 *__restrict__ onode;
+    const unsigned long long *__restrict__ omask;
+    double olo[3], osc[3];             // cell of x: floor((x - olo) * osc), clamped
+    double oext;                       // largest extent of the code space
     int n;                             // data vertices (ids >= n are super-simplex vertices)
     int nv, nt;
     int pmode;                         // PRED_*
-    int gdim[3];
-    double glo[3], ginv[3];
+    int gdim[3];                       // query bucketing: cell of x along axis a is
+    double glo[3], ginv[3];            // (x - glo) * ginv / gdim of the data bounding box
 };
 
 __device__ __forceinline__ int comp(const int4 &v, int i) {
@@ -107,16 +127,24 @@ __device__ __forceinline__ dv3 cload(const d4 *p) {
     return dv3{v.x, v.y, v.z};
 }
 
-__device__ __forceinline__ int seed_cell(const MeshView &M, dv3 q) {
-    double c[3] = {q.x, q.y, q.z};
-    int idx[3];
-#pragma unroll
-    for (int a = 0; a < 3; a++) {
-        double f = (c[a] - M.glo[a]) * M.ginv[a];
-        int k = (f >= 0.0) ? (f < (double)M.gdim[a] ? (int)f : M.gdim[a] - 1) : 0;
-        idx[a] = k;
-    }
-    return (idx[2] * M.gdim[1] + idx[1]) * M.gdim[0] + idx[0];
+// Squared distance between a tet centroid and q as natinterp3d's k-d tree
+// evaluates it: dist_sq = 0; dist_sq += SQ(node->pos[i] - pos[i]) for
+// i = 0, 1, 2 (kdtree.c:411-414; 0 + a == a exactly).
+__device__ __forceinline__ double kd_dist2(const d4 &c, const dv3 &q) {
+    const double dx = fsub(c.x, q.x), dy = fsub(c.y, q.y), dz = fsub(c.z, q.z);
+    return fadd(fadd(fmul(dx, dx), fmul(dy, dy)), fmul(dz, dz));
+}
+
+// A lower bound of kd_dist2 over every centroid inside the box [lo, hi]:
+// per axis the rounded distance to the nearer face (0 inside), squared and
+// summed in the same order.  Rounding is monotonic, so no centroid in the
+// box evaluates below it.
+__device__ __forceinline__ double box_dist2(const float4 &lo, const float4 &hi, const dv3 &q) {
+    auto axis = [](double x, float l, float h) {
+        return x < (double)l ? fsub((double)l, x) : (x > (double)h ? fsub(x, (double)h) : 0.0);
+    };
+    const double ax = axis(q.x, lo.x, hi.x), ay = axis(q.y, lo.y, hi.y), az = axis(q.z, lo.z, hi.z);
+    return fadd(fadd(fmul(ax, ax), fmul(ay, ay)), fmul(az, az));
 }
 
 // Lane helpers for a group of G consecutive lanes of a warp.
@@ -146,7 +174,186 @@ struct Grp {
     __device__ __forceinline__ int shfl_xor(int v, int off) const {
         return __shfl_xor_sync(mask, v, off, G);
     }
+    __device__ __forceinline__ double shfl_xor_d(double v, int off) const {
+        return __shfl_xor_sync(mask, v, off, G);
+    }
 };
+
+__device__ __forceinline__ unsigned long long spread3_64(unsigned v) {  // 20 bits -> every third bit
+    unsigned long long x = v & 0xfffffu;
+    x = (x | x << 32) & 0x1f00000000ffffull;
+    x = (x | x << 16) & 0x1f0000ff0000ffull;
+    x = (x | x << 8) & 0x100f00f00f00f00full;
+    x = (x | x << 4) & 0x10c30c30c30c30c3ull;
+    x = (x | x << 2) & 0x1249249249249249ull;
+    return x;
+}
+
+// cell coordinates (clamped) and 60-bit Morton code of a point in the
+// centroid code space
+__device__ __forceinline__ unsigned long long oct_code(const MeshView &M, const dv3 &p, int ix[3]) {
+    const double c[3] = {p.x, p.y, p.z};
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        const double f = (c[a] - M.olo[a]) * M.osc[a];
+        ix[a] = f > 0.0 ? (f < (double)((1 << OCT_BITS) - 1) ? (int)f : (1 << OCT_BITS) - 1) : 0;
+    }
+    return spread3_64(ix[0]) | (spread3_64(ix[1]) << 1) | (spread3_64(ix[2]) << 2);
+}
+
+// True when every point within sqrt(best) of q lies inside q's octree cell
+// at octree level 2 m (margins absorb the rounding of the cell bounds and of
+// the centroids' own cell assignment).
+__device__ __forceinline__ bool ball_in_cell(const MeshView &M, const dv3 &q, double best,
+                                             const int ix[3], int m) {
+    if (!(best < INFINITY)) return false;
+    const double r = sqrt(best) * (1.0 + 1e-9) + 1e-9 * M.oext;
+    const double c[3] = {q.x, q.y, q.z};
+    const int sh = OCT_BITS - 2 * m;
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        const double w = (double)(1 << sh) / M.osc[a];
+        const double lo = M.olo[a] + (double)(ix[a] >> sh) * w;
+        if (!(c[a] - r > lo && c[a] + r < lo + w)) return false;
+    }
+    return true;
+}
+
+// The tet whose centroid is nearest to q under kd_dist2, ties to the lowest
+// tet id: the seed natinterp3d's k-d tree returns (kd_nearest3_data,
+// kdtree.c:543-564).  Its pruning never skips a strictly nearer centroid, so
+// it returns a minimiser of the same rounded distance; among exactly equal
+// distances its visiting order decides, here the lowest id.
+// Bottom-up over the octree, one lane per child (two per lane for 64):
+//   1. descend along q's own code to the deepest node holding q's cell;
+//   2. search that node's subtree;
+//   3. walk back up: stop as soon as the ball of radius sqrt(best) around q
+//      lies inside the cell just searched (octree cells are disjoint, so no
+//      other centroid can be nearer); otherwise search the parent's other
+//      children.
+// A subtree search is depth-first, entering a child while its box bound is
+// <= best (an equal distance may still lose to a lower id).  stk: 64 ints of
+// group scratch (the descent path and the search frames); every lane keeps
+// the same control state and lane 0 stores it.  Bounded by SEED_STEP_LIMIT
+// visits (then the best centroid so far, a valid seed for the walk).
+template <int G>
+__device__ int nearest_centroid(const MeshView &M, const dv3 q, const Grp<G> &g, int *stk) {
+    static_assert(G == 32, "two children of a 64-wide node per lane");
+    int *path = stk;        // [OCT_KMAX + 1]
+    int *frm = stk + 16;    // 3 ints a frame: node, pending children (lo, hi word)
+    int ix[3];
+    const unsigned long long code = oct_code(M, q, ix);
+    int node = 0, depth = 0;
+    if (g.lane == 0) path[0] = 0;
+    for (; depth < OCT_KMAX; depth++) {
+        const int nch = __float_as_int(M.onode[2 * node + 1].w);
+        if (nch <= 0) break;
+        const unsigned long long mask = M.omask[node];
+        const int dg = (int)((code >> (6 * (OCT_KMAX - 1 - depth))) & 63ull);
+        if (!((mask >> dg) & 1ull)) break;
+        node = __float_as_int(M.onode[2 * node].w) + __popcll(mask & ((1ull << dg) - 1ull));
+        if (g.lane == 0) path[depth + 1] = node;
+    }
+    g.sync();
+    double best = INFINITY;
+    int bid = INT_MAX;
+    int steps = 0;
+    // centroids [a, a + n) of a leaf
+    auto leaf_pass = [&](int a, int n) {
+        for (int k0 = a; k0 < a + n; k0 += G) {
+            const int k = k0 + g.lane;
+            double d = INFINITY;
+            int id = INT_MAX;
+            if (k < a + n) {
+                const d4 e = M.cs[k];
+                d = kd_dist2(e, q);
+                id = (int)e.w;
+            }
+            const bool better = d < best || (d == best && id < bid);
+            if (g.any(better)) {
+                double bd = better ? d : best;
+                int bi = better ? id : bid;
+#pragma unroll
+                for (int off = G / 2; off > 0; off >>= 1) {
+                    const double od = g.shfl_xor_d(bd, off);
+                    const int oi = g.shfl_xor(bi, off);
+                    if (od < bd || (od == bd && oi < bi)) {
+                        bd = od;
+                        bi = oi;
+                    }
+                }
+                best = bd;
+                bid = bi;
+            }
+        }
+    };
+    // every centroid under node r, except under its child `skip`
+    auto subtree = [&](int r, int skip) {
+        {
+            const float4 lo = M.onode[2 * r], hi = M.onode[2 * r + 1];
+            if (__float_as_int(hi.w) <= 0) {
+                ++steps;
+                leaf_pass(__float_as_int(lo.w), -__float_as_int(hi.w));
+                return;
+            }
+        }
+        int sp = 1;
+        if (g.lane == 0) frm[0] = r;
+        bool fresh = true;
+        unsigned long long pend = 0;
+        while (sp > 0 && steps < SEED_STEP_LIMIT) {
+            ++steps;
+            g.sync();
+            const int nd = frm[3 * (sp - 1)];
+            if (!fresh)
+                pend = (unsigned long long)(unsigned)frm[3 * (sp - 1) + 1] |
+                       ((unsigned long long)(unsigned)frm[3 * (sp - 1) + 2] << 32);
+            const int first = __float_as_int(M.onode[2 * nd].w);
+            const int nch = __float_as_int(M.onode[2 * nd + 1].w);
+            // box bounds of the children lane and lane + 32
+            double d0 = INFINITY, d1 = INFINITY;
+            const int c0 = first + g.lane, c1 = first + 32 + g.lane;
+            if (g.lane < nch && c0 != skip) d0 = box_dist2(M.onode[2 * c0], M.onode[2 * c0 + 1], q);
+            if (32 + g.lane < nch && c1 != skip) d1 = box_dist2(M.onode[2 * c1], M.onode[2 * c1 + 1], q);
+            auto within = [&]() {
+                return (unsigned long long)g.ballot(d0 <= best) |
+                       ((unsigned long long)g.ballot(d1 <= best) << 32);
+            };
+            pend = fresh ? within() : (pend & within());
+            fresh = false;
+            bool pushed = false;
+            while (pend && steps < SEED_STEP_LIMIT) {
+                const int c = __ffsll((long long)pend) - 1;
+                pend &= pend - 1ull;
+                const int ch = first + c;
+                const float4 clo = M.onode[2 * ch], chi = M.onode[2 * ch + 1];
+                ++steps;
+                if (__float_as_int(chi.w) <= 0) {
+                    leaf_pass(__float_as_int(clo.w), -__float_as_int(chi.w));
+                    pend &= within();  // the same children, against the improved best
+                } else {
+                    if (g.lane == 0) {
+                        frm[3 * (sp - 1) + 1] = (int)(unsigned)pend;
+                        frm[3 * (sp - 1) + 2] = (int)(unsigned)(pend >> 32);
+                        frm[3 * sp] = ch;
+                    }
+                    ++sp;
+                    fresh = true;
+                    pushed = true;
+                    break;
+                }
+            }
+            if (!pushed) --sp;
+        }
+        g.sync();
+    };
+    subtree(node, -1);
+    for (int l = depth - 1; l >= 0; l--) {
+        if (ball_in_cell(M, q, best, ix, l + 1)) break;
+        subtree(path[l], path[l + 1]);
+    }
+    return bid == INT_MAX ? 0 : bid;
+}
 
 // Per-group scratch.  The first union member is live during the cavity
 // search, the second only during the single-lane replay of natinterp3d's
@@ -374,7 +581,8 @@ __device__ RowInfo sibson_row(const MeshView &M, const dv3 q, W &ws, const Grp<G
     bool on_face = false;  // PRED_EXACT: a face test of the located tet is exactly zero
 
     // ---- 1. point location -------------------------------------------------
-    int t = M.grid[seed_cell(M, q)];
+    // seed: the nearest tet centroid, then natinterp3d's walk
+    int t = nearest_centroid<G>(M, q, g, reinterpret_cast<int *>(ws.acc));
     for (;;) {
         if (r.steps >= WALK_LIMIT) {
             r.status = ST_WALK;

@@ -64,7 +64,8 @@ class DeviceMesh:
                     'nif_dmesh_create')
         info = (ctypes.c_int64 * 8)()
         N.check(self._lib.nif_dmesh_info(self._h, info), 'nif_dmesh_info')
-        self.grid_dims = (info[2], info[3], info[4])
+        # octree over the tet centroids (point-location seeds): nodes, node levels
+        self.octree_stats = {'nodes': int(info[2]), 'levels': int(info[3])}
         # tets whose orient3dfast sign the error bound cannot certify, and
         # those whose "> 0" flag the exact sign changes
         self.orientation_stats = {'uncertain': int(info[5]), 'flipped': int(info[6])}
@@ -152,7 +153,8 @@ class DeviceMesh:
             vals = torch.empty(max(nnz, 1), dtype=vals_dtype, device=self.device)[:nnz]
             totals = torch.empty(max(M, 1), dtype=torch.float64, device=self.device)[:M] \
                 if return_totals else None
-            N.check(self._lib.nif_weights_fill(self._h, M, _vp(ws), ws.numel(), _vp(rowptr),
+            N.check(self._lib.nif_weights_fill(self._h, _vp(q), _DT[q.dtype], M, cen, _vp(ws),
+                                               ws.numel(), _vp(rowptr),
                                                _vp(vals), _DT[vals_dtype], _vp(cols), _vp(totals),
                                                _stream_ptr(self.device)), 'nif_weights_fill')
         out = (rowptr, cols, vals)
@@ -203,21 +205,30 @@ class DeviceMesh:
             return out, summ.as_dict()
         return out
 
+    def pending_summary(self, pending, stream=None):
+        """Row counters of one interpolate(..., sync=False) call, read through
+        ``stream`` (a torch.cuda.Stream ordered after the call; default: the
+        current stream), which is the only stream this waits for.  Afterwards
+        the call's workspace may be released."""
+        M, ws = pending
+        summ = N.Summary()
+        sp = ctypes.c_void_p(stream.cuda_stream) if stream is not None else _stream_ptr(self.device)
+        N.check(self._lib.nif_query_summary(self._h, int(M), N.NIF_MODE_INTERP, _vp(ws),
+                                            ws.numel(), sp, ctypes.byref(summ)), 'nif_query_summary')
+        return summ.as_dict()
+
     def raise_pending(self, pending):
-        """Read the row counters of interpolate(..., sync=False) calls (after they
-        ran), keep their sum as ``last_summary`` and raise if any row failed."""
+        """Row counters of interpolate(..., sync=False) calls (pending handles,
+        read here after the calls ran, or dicts from :meth:`pending_summary`):
+        keep their sum as ``last_summary`` and raise if any row failed."""
         total = None
-        for M, ws in pending:
-            summ = N.Summary()
-            N.check(self._lib.nif_query_summary(self._h, int(M), N.NIF_MODE_INTERP, _vp(ws),
-                                                ws.numel(), _stream_ptr(self.device),
-                                                ctypes.byref(summ)), 'nif_query_summary')
-            d = summ.as_dict()
+        for item in pending:
+            d = item if isinstance(item, dict) else self.pending_summary(item)
             total = d if total is None else {k: (v + d[k] if k != 'first_status' else v or d[k])
                                              for k, v in total.items()}
-            self._raise_rows(summ)
         if total is not None:
             self.last_summary = total
+            self._raise_rows(N.Summary.from_dict(total))
 
     # -------------------------------------------------------------- sparse / grad
     def spmm(self, rowptr, cols, vals, x):

@@ -155,6 +155,43 @@ class Interpolator:
         z = np.load(path)
         return cls.from_mesh(z['centroid'], z['vxyz'], z['tet_v'], z['tet_n'], device=device)
 
+    # ------------------------------------------------------------------ pickling
+    def __getstate__(self):
+        """The key centroid and the packed mesh (natinterp3d's own mesh,
+        perturbations included), the predicate mode and launch settings; the
+        device-resident copy is rebuilt on first use after unpickling.  The
+        CUDA device is kept as its index (the current device where it does
+        not exist)."""
+        vxyz, tet_v, tet_n = self.mesh_arrays
+        dev = self._device_arg
+        if isinstance(dev, torch.device):
+            dev = dev.index
+        elif isinstance(dev, str):
+            dev = torch.device(dev).index
+        return {'format': 1, 'centroid': self._centroid, 'vxyz': vxyz, 'tet_v': tet_v,
+                'tet_n': tet_n, 'parallel': self.parallel, 'num_threads': self.num_threads,
+                'degeneracies': self.degeneracies, 'predicates': self._predicates,
+                'tuning': getattr(self, '_tuning', None), 'device': dev}
+
+    def __setstate__(self, state):
+        if state.get('format') != 1:
+            raise ValueError('unknown Interpolator pickle format %r' % (state.get('format'),))
+        dev = state['device']
+        if dev is not None and not (torch.cuda.is_available() and dev < torch.cuda.device_count()):
+            dev = None
+        self._centroid = np.asarray(state['centroid'], np.float64).reshape(3)
+        self.mesh_arrays = (np.ascontiguousarray(state['vxyz'], np.float64),
+                            np.ascontiguousarray(state['tet_v'], np.int32),
+                            np.ascontiguousarray(state['tet_n'], np.int32))
+        self.n_keys = self.mesh_arrays[0].shape[0] - 4
+        self.parallel, self.num_threads = state['parallel'], state['num_threads']
+        self.degeneracies = state['degeneracies']
+        self.host_mesh = None
+        self._device_arg = dev
+        self._dmesh = None
+        self._predicates = state['predicates']
+        self._tuning = state['tuning']
+
     @property
     def centroid(self):
         return self._centroid
@@ -272,17 +309,21 @@ class Interpolator:
         compute = torch.cuda.current_stream(dev)
         copy = torch.cuda.Stream(device=dev)
         staging = [torch.empty((PIPELINE_CHUNK, D), dtype=odt, pin_memory=True) for _ in range(2)]
-        failed = []
-        pending = None  # (slot, rows, device result, event)
+        counters = []
+        pending = None  # (slot, rows, device result, event, row-counter handle)
 
         def drain(item):
-            slot, (a, b), res, done = item
+            slot, (a, b), res, done, handle = item
             copy.wait_event(done)
             with torch.cuda.stream(copy):
                 staging[slot][:b - a].copy_(res.reshape(b - a, D), non_blocking=True)
                 res.record_stream(copy)
+                handle[1].record_stream(copy)
             copy.synchronize()
             out[a:b] = staging[slot][:b - a].numpy()
+            # the chunk's row counters, read on the copy stream (the compute
+            # stream runs on); its workspace is free once this returns
+            counters.append(dm.pending_summary(handle, copy))
 
         with torch.cuda.device(dev):
             for k, (a, b) in enumerate(bounds):
@@ -292,16 +333,16 @@ class Interpolator:
                     loaded.record(copy)
                 compute.wait_event(loaded)
                 qd.record_stream(compute)
-                res, summ = dm.interpolate(qd, vd, self._centroid, return_summary=True,
-                                           check=False, sync=False)
-                failed.append(summ)
+                res, handle = dm.interpolate(qd, vd, self._centroid, return_summary=True,
+                                             check=False, sync=False)
                 done = torch.cuda.Event()
                 done.record(compute)
                 if pending is not None:
                     drain(pending)
-                pending = (k % 2, (a, b), res, done)
+                pending = (k % 2, (a, b), res, done, handle)
             drain(pending)
-        dm.raise_pending(failed)
+            pending = None
+        dm.raise_pending(counters)
         return out[:, 0] if vd.dim() == 1 else out
 
     # -------------------------------------------------------- device-resident API
@@ -314,6 +355,17 @@ class Interpolator:
         if as_torch_csr:
             return torch.sparse_csr_tensor(rowptr, cols, vals, size=(queries.shape[0], self.n_keys))
         return rowptr, cols, vals
+
+    def get_weights_dlpack(self, queries: torch.Tensor, dtype=None):
+        """The device CSR of :meth:`get_weights_device` as three DLPack
+        capsules (indptr int32 [M+1], indices int32 [nnz], data [nnz]) for
+        other CUDA array libraries, with no copy: e.g. with CuPy,
+        ``cupyx.scipy.sparse.csr_matrix((cp.from_dlpack(data),
+        cp.from_dlpack(indices), cp.from_dlpack(indptr)), shape=(M, N))``.
+        Columns within a row are in natinterp3d's order."""
+        from torch.utils.dlpack import to_dlpack
+        rowptr, cols, vals = self.get_weights_device(queries, dtype=dtype)
+        return to_dlpack(rowptr), to_dlpack(cols), to_dlpack(vals)
 
     def interpolate_device(self, queries: torch.Tensor, values: torch.Tensor, check=True):
         return self.device_mesh.interpolate(queries, values, self._centroid, check=check)

@@ -23,7 +23,6 @@ LIB_DIR = os.path.join(HERE, 'lib')
 REF_DIR = os.path.join(HERE, '_ref')
 ORACLE_SO = os.path.join(LIB_DIR, 'libnif_oracle.so')
 REF_SO = os.path.join(REF_DIR, 'libnatinterp3d_ref.so')
-DEFAULT_REF_SRC = '/root/reference/src/natinterp3d'
 
 # natinterp3d's Linux flags (setup.py:17-22, 36)
 REF_CFLAGS = ['-std=c11', '-O3', '-fno-math-errno', '-flto', '-fopenmp',
@@ -32,7 +31,11 @@ REF_LDFLAGS = ['-fopenmp', '-flto', '-lm', '-lpthread']
 
 
 def ref_source_dir():
-    return os.environ.get('NATINTERP3D_SRC', DEFAULT_REF_SRC)
+    """natinterp3d's C sources, located as the product's build recipe does
+    (NATINTERP3D_SRC, an importable natinterp3d package, the default checkout)."""
+    sys.path.insert(0, os.path.dirname(HERE))
+    from natinterp3d_b200 import _build
+    return _build.ref_source_dir()
 
 
 def _cc():

@@ -1,5 +1,5 @@
 """The sharding helpers over NCCL with the CUDA interpolator, world size 1
-(each gpurun call has one GPU; the two-rank host logic is tested with gloo on
+(the GPU tests run on one GPU; the two-rank host logic is tested with gloo on
 CPU in test_sharding_gloo.py)."""
 import socket
 

@@ -42,24 +42,73 @@ def _call_noalloc(dm, q, v, centroid, out, summary=None):
                                        ctypes.byref(summary) if summary is not None else None)
 
 
-@pytest.mark.parametrize('values_dtype', [torch.float32, torch.float64])
-def test_noalloc_matches_workspace_entry_point_twice(values_dtype, cuda_device):
+@pytest.fixture(scope='module')
+def noalloc_mesh(cuda_device):
     rng = np.random.default_rng(11)
     keys = rng.uniform(0.0, 1.0, (20000, 3))
     c = keys.mean(axis=0)
-    host = HostMesh(keys - c)
-    dm = DeviceMesh(*host.export(), device=cuda_device)
-    q = torch.from_numpy(rng.uniform(0.02, 0.98, (60000, 3))).to(cuda_device)
-    v = torch.from_numpy(rng.standard_normal((20000, 3))).to(cuda_device, values_dtype)
+    dm = DeviceMesh(*HostMesh(keys - c).export(), device=cuda_device)
+    return dm, c, rng
 
+
+def _out_dtype(q, v):
+    return torch.float32 if (q.dtype == torch.float32 and v.dtype == torch.float32) else torch.float64
+
+
+@pytest.mark.parametrize('query_dtype', [torch.float32, torch.float64])
+@pytest.mark.parametrize('values_dtype', [torch.float32, torch.float64])
+def test_noalloc_matches_workspace_entry_point_twice(query_dtype, values_dtype, noalloc_mesh,
+                                                     cuda_device):
+    dm, c, rng = noalloc_mesh
+    q = torch.from_numpy(rng.uniform(0.02, 0.98, (60000, 3))).to(cuda_device, query_dtype)
+    v = torch.from_numpy(rng.standard_normal((20000, 3))).to(cuda_device, values_dtype)
     expect = dm.interpolate(q, v, c).cpu().numpy()
     for _ in range(2):
-        out = torch.full((q.shape[0], 3), float('nan'), dtype=torch.float64, device=cuda_device)
+        out = torch.full((q.shape[0], 3), float('nan'), dtype=_out_dtype(q, v), device=cuda_device)
         summ = N.Summary()
         assert _call_noalloc(dm, q, v, c, out, summ) == N.NIF_OK
         assert summ.rows_failed == 0
         got = out.cpu().numpy()
         assert np.array_equal(got, expect), np.nanmax(np.abs(got - expect))
+
+
+def test_noalloc_empty_call(noalloc_mesh, cuda_device):
+    dm, c, _ = noalloc_mesh
+    q = torch.empty((0, 3), dtype=torch.float64, device=cuda_device)
+    v = torch.zeros((20000, 2), dtype=torch.float64, device=cuda_device)
+    out = torch.empty((1, 2), dtype=torch.float64, device=cuda_device)
+    summ = N.Summary()
+    assert _call_noalloc(dm, q, v, c, out, summ) == N.NIF_OK
+    assert summ.rows_failed == 0 and summ.walk_steps == 0
+
+
+def test_noalloc_with_finer_bucketing(noalloc_mesh, cuda_device):
+    # a positive bucket_shift asks for more buckets than the fixed scratch
+    # holds; the call caps it and still returns the same bits
+    dm, c, rng = noalloc_mesh
+    q = torch.from_numpy(rng.uniform(0.02, 0.98, (300000, 3))).to(cuda_device)
+    v = torch.from_numpy(rng.standard_normal((20000, 1))).to(cuda_device)
+    expect = dm.interpolate(q, v, c).cpu().numpy()
+    old = dm.get_tuning()
+    dm.set_tuning({'blocks_per_sm': 6, 'bucket_shift': 1, 'tile': 16})
+    try:
+        for _ in range(2):
+            out = torch.full((q.shape[0], 1), float('nan'), dtype=torch.float64, device=cuda_device)
+            assert _call_noalloc(dm, q, v, c, out) == N.NIF_OK
+            assert np.array_equal(out.cpu().numpy(), expect)
+    finally:
+        dm.set_tuning(old)
+
+
+def test_noalloc_at_its_maximum_size(noalloc_mesh, cuda_device):
+    dm, c, rng = noalloc_mesh
+    q = torch.from_numpy(rng.uniform(0.02, 0.98, (MAX_QUERIES, 3))).to(cuda_device)
+    v = torch.from_numpy(rng.standard_normal((20000, 1))).to(cuda_device)
+    out = torch.empty((MAX_QUERIES, 1), dtype=torch.float64, device=cuda_device)
+    summ = N.Summary()
+    assert _call_noalloc(dm, q, v, c, out, summ) == N.NIF_OK
+    assert summ.rows_failed == 0
+    assert np.array_equal(out.cpu().numpy(), dm.interpolate(q, v, c).cpu().numpy())
 
 
 def test_noalloc_rejects_batches_beyond_its_fixed_scratch(cuda_device):
