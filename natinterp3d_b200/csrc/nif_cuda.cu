@@ -264,6 +264,30 @@ __global__ void k_cen_gather(MeshView M, const int32_t *__restrict__ idx, const 
     }
 }
 
+// cell of a centroid in the uniform seed grid (the formula grid_nearest uses)
+__device__ __forceinline__ int grid_cell(const MeshView &M, const d4 &c) {
+    const double x[3] = {c.x, c.y, c.z};
+    int ic[3];
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        const double f = (x[a] - M.glo[a]) * M.ginv[a];
+        ic[a] = f > 0.0 ? (f < (double)(M.gdim[a] - 1) ? (int)f : M.gdim[a] - 1) : 0;
+    }
+    return (ic[2] * M.gdim[1] + ic[1]) * M.gdim[0] + ic[0];
+}
+
+__global__ void k_grid_count(MeshView M, int *__restrict__ count) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < M.nt; k += gridDim.x * blockDim.x)
+        atomicAdd(&count[grid_cell(M, M.cs[k])], 1);
+}
+
+__global__ void k_grid_fill(MeshView M, int *__restrict__ cursor, d4 *__restrict__ items) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < M.nt; k += gridDim.x * blockDim.x) {
+        const d4 c = M.cs[k];
+        items[atomicAdd(&cursor[grid_cell(M, c)], 1)] = c;
+    }
+}
+
 // Octree build, one node level at a time.  Nodes are numbered level by level
 // in centroid order; node j spans centroids [na[j], nb[j]).  node_of[i] is
 // the deepest node built so far that holds centroid i.  A level-k node with
@@ -875,10 +899,14 @@ __device__ __forceinline__ void record(DevSummary *sum, const RowInfo &r, int la
 // PM_FILTER; OCC resident blocks per SM.  With tile == 0 group k takes rows
 // k, k + ng, k + 2 ng, ...; with tile > 0 it takes tiles of `tile`
 // consecutive rows from the device counter (zeroed before the launch).
-template <class QT, class Sink, int PM, int OCC>
+// With LOC the rows were located by k_locate: located[i] is row i's tet, -1
+// outside the super-simplex, -2 a walk that hit its step limit; the kernel
+// then holds no point-location code (a smaller instruction footprint).
+template <class QT, class Sink, int PM, int OCC, bool LOC>
 __global__ void __launch_bounds__(FAST_BLOCK, OCC) k_rows_fast(MeshView M, const QT *__restrict__ Q,
                                                           Centroid cen, const int *__restrict__ order,
                                                           int64_t nrows, const int *nrows_dev,
+                                                          const int *__restrict__ located,
                                                           Sink sink, LargeQueue lq,
                                                           DevSummary *sum, int tile,
                                                           unsigned long long *counter) {
@@ -906,7 +934,17 @@ __global__ void __launch_bounds__(FAST_BLOCK, OCC) k_rows_fast(MeshView M, const
         }
         const int64_t i = order[s];
         const dv3 q = load_query(Q, i, cen.c);
-        const RowInfo r = sibson_row<G, FastWS, Sink::FULL, PM>(M, q, ws, g);
+        RowInfo r;
+        if constexpr (LOC) {
+            const int t = located[i];
+            if (t >= 0) {
+                r = sibson_row<G, FastWS, Sink::FULL, PM, true>(M, q, ws, g, nullptr, t);
+            } else {
+                r = RowInfo{t == -2 ? ST_WALK : ST_OK, 0, 0, t == -1, false, 0.0, 0, 0, 0, 0, 0};
+            }
+        } else {
+            r = sibson_row<G, FastWS, Sink::FULL, PM>(M, q, ws, g);
+        }
         steps += r.steps;
         if (r.status == ST_CAPACITY || r.status == ST_UNCERTAIN) {
             if (g.lane == 0) {
@@ -921,6 +959,46 @@ __global__ void __launch_bounds__(FAST_BLOCK, OCC) k_rows_fast(MeshView M, const
             record<G>(sum, r, g.lane);
             sink.template emit<G>(i, r.status == ST_OK ? r.nnb : 0, ws, g, false, M, q, r);
         }
+        g.sync();
+        s += tile <= 0 ? ng : 1;
+    }
+    if (g.lane == 0 && steps) atomicAdd(&sum->walk_steps, steps);
+}
+
+// Point location of every row (natinterp3d's signs): one warp per row, rows
+// in bucket order as k_rows_fast takes them; located[i] = the tet, -1
+// outside the super-simplex, -2 a walk that hit its step limit.
+template <class QT>
+__global__ void __launch_bounds__(FAST_BLOCK) k_locate(MeshView M, const QT *__restrict__ Q, Centroid cen,
+                                                       const int *__restrict__ order, int64_t nrows,
+                                                       int *__restrict__ located, DevSummary *sum,
+                                                       int tile, unsigned long long *counter) {
+    constexpr int G = 32;
+    constexpr int GPB = FAST_BLOCK / G;
+    __shared__ int scratch[GPB][64];
+    Grp<G> g;
+    int *scr = scratch[threadIdx.x / G];
+    const int64_t gid = tile <= 0 ? (int64_t)blockIdx.x * GPB + threadIdx.x / G : 0;
+    const int64_t ng = (int64_t)gridDim.x * GPB;
+    unsigned long long steps = 0;
+    int64_t s = gid, s1 = tile <= 0 ? nrows : 0;
+    for (;;) {
+        if (s >= s1) {
+            if (tile <= 0) break;
+            unsigned long long t = 0;
+            if (g.lane == 0) t = atomicAdd(counter, 1ull);
+            t = __shfl_sync(g.mask, t, 0, G);
+            s = (int64_t)t * tile;
+            if (s >= nrows) break;
+            s1 = min(nrows, s + (int64_t)tile);
+        }
+        const int64_t i = order[s];
+        const dv3 q = load_query(Q, i, cen.c);
+        RowInfo r{ST_OK, 0, 0, false, false, 0.0, 0, 0, 0, 0, 0};
+        bool on_face = false;
+        const int t = locate<G, PM_PLAIN>(M, q, g, scr, r, on_face);
+        steps += r.steps;
+        if (g.lane == 0) located[i] = r.status != ST_OK ? -2 : (r.outside ? -1 : t);
         g.sync();
         s += tile <= 0 ? ng : 1;
     }
@@ -1066,6 +1144,13 @@ inline int cuda_rc(cudaError_t e) { return e == cudaSuccess ? NIF_OK : NIF_ERR_C
 // the room, its nodes stay leaves -- larger leaves, same results.
 int oct_node_cap(int nt) { return nt / 8 + 1024; }
 
+// Seed-grid cells per tet (about two centroids a cell), and the cells the
+// resident mesh has room for.
+#ifndef NIF_GRID_CELLS_PER_TET
+#define NIF_GRID_CELLS_PER_TET 0.5
+#endif
+int grid_cell_cap(int nt) { return (int)(NIF_GRID_CELLS_PER_TET * nt) + 64; }
+
 // Scratch of the centroid sort and octree build at mesh creation, carved
 // from the start of the face-circumcentre array (filled only afterwards).
 struct OctScratch {
@@ -1076,6 +1161,7 @@ struct OctScratch {
     unsigned long long *code;
     int *node_of, *flag, *scan;
     int *na, *nb, *par, *first, *nch;
+    int *gcursor;
 };
 
 OctScratch carve_oct_scratch(Carve &c, int nt) {
@@ -1101,6 +1187,7 @@ OctScratch carve_oct_scratch(Carve &c, int nt) {
     S.par = c.take<int>(cap);
     S.first = c.take<int>(cap);
     S.nch = c.take<int>(cap);
+    S.gcursor = c.take<int>(grid_cell_cap(nt));
     return S;
 }
 
@@ -1121,6 +1208,8 @@ struct MeshLayout {
     d4 *cs;                      // sorted centroids
     float4 *onode;               // octree node records, two float4 each
     unsigned long long *omask;   // octree child digits
+    int *gstart;                 // seed grid: cell starts
+    d4 *gitems;                  // seed grid: centroids by cell
     double *bbox_part;
     int *flag;
 };
@@ -1136,6 +1225,8 @@ MeshLayout carve_mesh(Carve &c, int nv, int nt) {
     L.cs = c.take<d4>(nt);
     L.onode = c.take<float4>(2 * (size_t)oct_node_cap(nt));
     L.omask = c.take<unsigned long long>(oct_node_cap(nt));
+    L.gstart = c.take<int>(grid_cell_cap(nt) + 1);
+    L.gitems = c.take<d4>(nt);
     L.bbox_part = c.take<double>(6 * 256);
     L.flag = c.take<int>(4);
     return L;
@@ -1158,6 +1249,7 @@ struct QueryLayout {
     int64_t *scan_total;
     LargeWS *large_ws;
     double *exact;          // NIF_EXACT_SCRATCH doubles per large-row group
+    int *located;           // k_locate's tet per row (null: the row kernel locates)
     // weights mode only
     int *cnt;
     uint8_t *staged;
@@ -1193,6 +1285,7 @@ QueryLayout carve_query(Carve &c, int64_t M, int mode) {
     L.scan_total = c.take<int64_t>(1);
     L.large_ws = c.take<LargeWS>(LARGE_GROUPS);
     L.exact = c.take<double>((size_t)LARGE_GROUPS * NIF_EXACT_SCRATCH);
+    L.located = c.take<int>(M > 0 ? M : 1);
     if (mode == NIF_MODE_WEIGHTS) {
         const int64_t m1 = M > 0 ? M : 1;
         L.cnt = c.take<int>(m1);
@@ -1303,49 +1396,91 @@ struct RowSet {
     int *large;
     DevSummary *sum;
     unsigned long long *counter;
+    const int *located;  // k_locate's tets of these rows, or null (the row kernel locates)
 };
 
 inline RowSet all_rows(const QueryLayout &L) {
-    return RowSet{L.order, nullptr, L.large_list, L.sum, L.counter};
+    return RowSet{L.order, nullptr, L.large_list, L.sum, L.counter, L.located};
+}
+
+// queries per work item of the tiled schedule: at most `tile`, smaller for a
+// call too small to give every resident group two tiles
+inline int fit_tile(int tile, int64_t M, int per_sm, int num_sms, int gpb) {
+    if (tile > 0) {
+        const int64_t fit = M / (2 * (int64_t)per_sm * num_sms * gpb);
+        if (fit < tile) tile = (int)fit;
+    }
+    return tile;
 }
 
 // persistent grid of the fast row kernel: resident blocks per SM x SMs
-template <class QT, class Sink, int PM, int OCC>
+template <class QT, class Sink, int PM, int OCC, bool LOC>
 void launch_fast_occ(const nif_dmesh *m, const QT *Q, int64_t M, const Centroid &cen,
                      const RowSet &R, const Sink &sink, cudaStream_t st) {
     constexpr int GPB = FAST_BLOCK / FAST_G;
     const size_t smem = GPB * sizeof(FastWS);
-    auto kern = k_rows_fast<QT, Sink, PM, OCC>;
+    auto kern = k_rows_fast<QT, Sink, PM, OCC, LOC>;
     const int per_sm = resident_blocks(kern, FAST_BLOCK, smem);
     // tile is an upper bound: a call too small to give every resident group
     // two tiles takes smaller ones (or the static stride), so that small
     // calls keep the whole GPU busy
-    int tile = m->tune.tile;
-    if (tile > 0) {
-        const int64_t fit = M / (2 * (int64_t)per_sm * m->num_sms * GPB);
-        if (fit < tile) tile = (int)fit;
-    }
+    const int tile = fit_tile(m->tune.tile, M, per_sm, m->num_sms, GPB);
     int64_t blocks = (M + GPB - 1) / GPB;
     if (tile > 0) blocks = (M + (int64_t)GPB * tile - 1) / ((int64_t)GPB * tile);
     const int64_t cap = (int64_t)per_sm * m->num_sms;
     if (blocks > cap) blocks = cap;
     if (blocks < 1) blocks = 1;
     if (tile > 0) cudaMemsetAsync(R.counter, 0, sizeof(unsigned long long), st);
-    kern<<<(unsigned)blocks, FAST_BLOCK, smem, st>>>(m->view, Q, cen, R.order, M, R.nrows_dev, sink,
-                                                    LargeQueue{R.large}, R.sum, tile, R.counter);
+    kern<<<(unsigned)blocks, FAST_BLOCK, smem, st>>>(m->view, Q, cen, R.order, M, R.nrows_dev,
+                                                    R.located, sink, LargeQueue{R.large}, R.sum, tile,
+                                                    R.counter);
+}
+
+// k_locate over the rows of R (all of them: located rows are never a queue)
+template <class QT>
+void launch_locate(const nif_dmesh *m, const QT *Q, int64_t M, const Centroid &cen, const RowSet &R,
+                   int *located, cudaStream_t st) {
+    constexpr int GPB = FAST_BLOCK / 32;
+    auto kern = k_locate<QT>;
+    const int per_sm = resident_blocks(kern, FAST_BLOCK, 0);
+    const int tile = fit_tile(m->tune.tile, M, per_sm, m->num_sms, GPB);
+    int64_t blocks = (M + GPB - 1) / GPB;
+    if (tile > 0) blocks = (M + (int64_t)GPB * tile - 1) / ((int64_t)GPB * tile);
+    const int64_t cap = (int64_t)per_sm * m->num_sms;
+    if (blocks > cap) blocks = cap;
+    if (blocks < 1) blocks = 1;
+    if (tile > 0) cudaMemsetAsync(R.counter, 0, sizeof(unsigned long long), st);
+    kern<<<(unsigned)blocks, FAST_BLOCK, 0, st>>>(m->view, Q, cen, R.order, M, located, R.sum, tile,
+                                                 R.counter);
 }
 
 // the structure-only (gradient) rows keep their own occupancy; the others
 // run at the mesh's tuned one
+template <class QT, class Sink, int PM, bool LOC>
+void launch_fast_loc(const nif_dmesh *m, const QT *Q, int64_t M, const Centroid &cen,
+                     const RowSet &R, const Sink &sink, cudaStream_t st) {
+    if constexpr (!Sink::FULL)
+        launch_fast_occ<QT, Sink, PM, Sink::MIN_BLOCKS, LOC>(m, Q, M, cen, R, sink, st);
+    else if (m->tune.blocks_per_sm == OCC_LO)
+        launch_fast_occ<QT, Sink, PM, OCC_LO, LOC>(m, Q, M, cen, R, sink, st);
+    else
+        launch_fast_occ<QT, Sink, PM, OCC_HI, LOC>(m, Q, M, cen, R, sink, st);
+}
+
+// With natinterp3d's signs and a located[] array in R (whose rows are a
+// plain order, not a queue), the rows are located by k_locate first and the
+// row kernel starts at the cavity; otherwise the row kernel locates.
 template <class QT, class Sink, int PM>
 void launch_fast(const nif_dmesh *m, const QT *Q, int64_t M, const Centroid &cen,
                  const RowSet &R, const Sink &sink, cudaStream_t st) {
-    if constexpr (!Sink::FULL)
-        launch_fast_occ<QT, Sink, PM, Sink::MIN_BLOCKS>(m, Q, M, cen, R, sink, st);
-    else if (m->tune.blocks_per_sm == OCC_LO)
-        launch_fast_occ<QT, Sink, PM, OCC_LO>(m, Q, M, cen, R, sink, st);
-    else
-        launch_fast_occ<QT, Sink, PM, OCC_HI>(m, Q, M, cen, R, sink, st);
+    if constexpr (PM == PM_PLAIN) {
+        if (R.located && !R.nrows_dev) {
+            launch_locate(m, Q, M, cen, R, const_cast<int *>(R.located), st);
+            launch_fast_loc<QT, Sink, PM, true>(m, Q, M, cen, R, sink, st);
+            return;
+        }
+    }
+    launch_fast_loc<QT, Sink, PM, false>(m, Q, M, cen, R, sink, st);
 }
 
 // fast rows (filtered when the mesh's predicate mode is not the default),
@@ -1368,7 +1503,8 @@ template <class QT, class Sink>
 void refill_rows(const nif_dmesh *m, const QT *Q, int64_t M, const Centroid &cen, const QueryLayout &L,
                  const Sink &sink, cudaStream_t st) {
     // fast-kernel rows longer than ROW_STAGE: the queue's length is on the device
-    const RowSet R{L.refill, &L.sum->refill_count, L.large_list, L.fill_sum, L.counter};
+    // (few rows: the row kernel locates them itself)
+    const RowSet R{L.refill, &L.sum->refill_count, L.large_list, L.fill_sum, L.counter, nullptr};
     if (m->view.pmode == PRED_FAST)
         launch_fast<QT, Sink, PM_PLAIN>(m, Q, M, cen, R, sink, st);
     else
@@ -1478,6 +1614,8 @@ NIF_EXPORT int nif_dmesh_create(const double *d_vxyz, const int32_t *d_tet_v,
     V.cs = L.cs;
     V.onode = L.onode;
     V.omask = L.omask;
+    V.gstart = L.gstart;
+    V.gitems = L.gitems;
 
     int rc = NIF_OK;
     do {
@@ -1509,11 +1647,29 @@ NIF_EXPORT int nif_dmesh_create(const double *d_vxyz, const int32_t *d_tet_v,
         for (int a = 0; a < 3; a++)
             if (ext[a] < emax * 1e-3) ext[a] = emax * 1e-3;
 
-        // query bucketing normalises by the data bounding box
-        for (int a = 0; a < 3; a++) {
-            V.gdim[a] = 1;
-            V.glo[a] = lo[a];
-            V.ginv[a] = 1.0 / ext[a];
+        // seed grid over the data bounding box, about two centroids a cell,
+        // within the room grid_cell_cap(n_tets) leaves; query bucketing
+        // normalises by the same box
+        {
+            const int cap = grid_cell_cap(n_tets);
+            const double side = cbrt(ext[0] * ext[1] * ext[2] / (NIF_GRID_CELLS_PER_TET * n_tets));
+            int gd[3];
+            for (int a = 0; a < 3; a++) {
+                const double r = ext[a] / side;
+                gd[a] = r < 1.0 ? 1 : (r > 4096.0 ? 4096 : (int)(r + 0.5));
+            }
+            while ((int64_t)gd[0] * gd[1] * gd[2] > cap) {
+                const int a = (gd[0] >= gd[1] && gd[0] >= gd[2]) ? 0 : (gd[1] >= gd[2] ? 1 : 2);
+                gd[a] = gd[a] > 1 ? gd[a] - 1 : 1;
+            }
+            V.gext = 0.0;
+            for (int a = 0; a < 3; a++) {
+                V.gdim[a] = gd[a];
+                V.glo[a] = lo[a];
+                V.ginv[a] = (double)gd[a] / ext[a];
+                V.gh[a] = ext[a] / (double)gd[a];
+                V.gext = fmax(V.gext, ext[a]);
+            }
         }
         // centroid code space: the bounding box of all vertices (the
         // super-simplex's four included), which holds every tet centroid
@@ -1604,6 +1760,21 @@ NIF_EXPORT int nif_dmesh_create(const double *d_vxyz, const int32_t *d_tet_v,
                     lvl[l], lvl[l + 1], T.na, T.nb, T.first, T.nch, L.cs, L.onode);
             h->oct_nodes = lvl[levels];
             h->oct_levels = levels;
+            // seed grid: centroids counted per cell, cell starts scanned, then
+            // each centroid placed at its cell's cursor
+            const int ncell = V.gdim[0] * V.gdim[1] * V.gdim[2];
+            if (cudaMemsetAsync(L.gstart, 0, sizeof(int) * (ncell + 1), st) != cudaSuccess) {
+                rc = NIF_ERR_CUDA;
+                break;
+            }
+            k_grid_count<<<nb, 256, 0, st>>>(V, L.gstart);
+            launch_scan<int>(L.gstart, ncell, T.bsum, L.gstart + ncell, L.gstart, st);
+            if (cudaMemcpyAsync(T.gcursor, L.gstart, sizeof(int) * ncell, cudaMemcpyDeviceToDevice,
+                                st) != cudaSuccess) {
+                rc = NIF_ERR_CUDA;
+                break;
+            }
+            k_grid_fill<<<nb, 256, 0, st>>>(V, T.gcursor, L.gitems);
         }
         k_prep_geometry<<<blocks_for(n_tets, 128), 128, 0, st>>>(V, L.tinfo, L.tcc, L.fcc, L.flag);
         int flag[4];

@@ -21,90 +21,139 @@
 
 namespace nif {
 
-// value + derivative along x, y, z
-struct dual3 {
-    double v, dx, dy, dz;
+// A value and its derivatives along ND directions (ND = 3: x, y and z at
+// once; ND = 1: one direction per pass, a third of the live state).
+template <int ND>
+struct dualn {
+    double v, d[ND];
 };
 
-__device__ __forceinline__ dual3 dconst(double c) { return dual3{c, 0.0, 0.0, 0.0}; }
-
-__device__ __forceinline__ dual3 operator+(dual3 a, dual3 b) {
-    return dual3{fadd(a.v, b.v), a.dx + b.dx, a.dy + b.dy, a.dz + b.dz};
-}
-__device__ __forceinline__ dual3 operator-(dual3 a, dual3 b) {
-    return dual3{fsub(a.v, b.v), a.dx - b.dx, a.dy - b.dy, a.dz - b.dz};
-}
-__device__ __forceinline__ dual3 operator*(dual3 a, dual3 b) {
-    return dual3{fmul(a.v, b.v), a.v * b.dx + a.dx * b.v, a.v * b.dy + a.dy * b.v,
-                 a.v * b.dz + a.dz * b.v};
-}
-__device__ __forceinline__ dual3 operator/(dual3 a, dual3 b) {
-    const double q = fdiv(a.v, b.v);
-    const double r = 1.0 / b.v;
-    return dual3{q, (a.dx - q * b.dx) * r, (a.dy - q * b.dy) * r, (a.dz - q * b.dz) * r};
+template <int ND>
+__device__ __forceinline__ dualn<ND> dconst(double c) {
+    dualn<ND> r;
+    r.v = c;
+#pragma unroll
+    for (int i = 0; i < ND; i++) r.d[i] = 0.0;
+    return r;
 }
 
+template <int ND>
+__device__ __forceinline__ dualn<ND> operator+(dualn<ND> a, dualn<ND> b) {
+    dualn<ND> r;
+    r.v = fadd(a.v, b.v);
+#pragma unroll
+    for (int i = 0; i < ND; i++) r.d[i] = a.d[i] + b.d[i];
+    return r;
+}
+template <int ND>
+__device__ __forceinline__ dualn<ND> operator-(dualn<ND> a, dualn<ND> b) {
+    dualn<ND> r;
+    r.v = fsub(a.v, b.v);
+#pragma unroll
+    for (int i = 0; i < ND; i++) r.d[i] = a.d[i] - b.d[i];
+    return r;
+}
+template <int ND>
+__device__ __forceinline__ dualn<ND> operator*(dualn<ND> a, dualn<ND> b) {
+    dualn<ND> r;
+    r.v = fmul(a.v, b.v);
+#pragma unroll
+    for (int i = 0; i < ND; i++) r.d[i] = a.v * b.d[i] + a.d[i] * b.v;
+    return r;
+}
+template <int ND>
+__device__ __forceinline__ dualn<ND> operator/(dualn<ND> a, dualn<ND> b) {
+    dualn<ND> r;
+    r.v = fdiv(a.v, b.v);
+    const double inv = 1.0 / b.v;
+#pragma unroll
+    for (int i = 0; i < ND; i++) r.d[i] = (a.d[i] - r.v * b.d[i]) * inv;
+    return r;
+}
+
+template <int ND>
 struct dvec {
-    dual3 x, y, z;
+    dualn<ND> x, y, z;
 };
 
-__device__ __forceinline__ dvec dvconst(dv3 a) { return dvec{dconst(a.x), dconst(a.y), dconst(a.z)}; }
-__device__ __forceinline__ dvec dvsub(dvec a, dvec b) { return dvec{a.x - b.x, a.y - b.y, a.z - b.z}; }
-__device__ __forceinline__ dvec dvadd(dvec a, dvec b) { return dvec{a.x + b.x, a.y + b.y, a.z + b.z}; }
-__device__ __forceinline__ dvec dvscale(dvec a, dual3 s) { return dvec{a.x * s, a.y * s, a.z * s}; }
-__device__ __forceinline__ dvec dvcross(dvec b, dvec c) {
-    return dvec{b.y * c.z - b.z * c.y, b.z * c.x - b.x * c.z, b.x * c.y - b.y * c.x};
+template <int ND>
+__device__ __forceinline__ dvec<ND> dvconst(dv3 a) {
+    return dvec<ND>{dconst<ND>(a.x), dconst<ND>(a.y), dconst<ND>(a.z)};
 }
-__device__ __forceinline__ dual3 dvdot(dvec a, dvec b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+template <int ND>
+__device__ __forceinline__ dvec<ND> dvsub(dvec<ND> a, dvec<ND> b) {
+    return dvec<ND>{a.x - b.x, a.y - b.y, a.z - b.z};
+}
+template <int ND>
+__device__ __forceinline__ dvec<ND> dvadd(dvec<ND> a, dvec<ND> b) {
+    return dvec<ND>{a.x + b.x, a.y + b.y, a.z + b.z};
+}
+template <int ND>
+__device__ __forceinline__ dvec<ND> dvscale(dvec<ND> a, dualn<ND> s) {
+    return dvec<ND>{a.x * s, a.y * s, a.z * s};
+}
+template <int ND>
+__device__ __forceinline__ dvec<ND> dvcross(dvec<ND> b, dvec<ND> c) {
+    return dvec<ND>{b.y * c.z - b.z * c.y, b.z * c.x - b.x * c.z, b.x * c.y - b.y * c.x};
+}
+template <int ND>
+__device__ __forceinline__ dualn<ND> dvdot(dvec<ND> a, dvec<ND> b) {
+    return a.x * b.x + a.y * b.y + a.z * b.z;
+}
 
 // the same formulas and groupings as tri_cc / tet_cc / subcell_volume
-__device__ __forceinline__ dvec tri_cc_d(dvec a, dvec b, dvec c) {
-    dvec ab = dvsub(b, a), ac = dvsub(c, a);
-    dvec n = dvcross(ab, ac);
-    dual3 n2 = dvdot(n, n);
+template <int ND>
+__device__ __forceinline__ dvec<ND> tri_cc_d(dvec<ND> a, dvec<ND> b, dvec<ND> c) {
+    dvec<ND> ab = dvsub(b, a), ac = dvsub(c, a);
+    dvec<ND> n = dvcross(ab, ac);
+    dualn<ND> n2 = dvdot(n, n);
     if (n2.v < 1e-30) {
-        const dual3 three = dconst(3.0);
-        return dvec{(a.x + b.x + c.x) / three, (a.y + b.y + c.y) / three, (a.z + b.z + c.z) / three};
+        const dualn<ND> three = dconst<ND>(3.0);
+        return dvec<ND>{(a.x + b.x + c.x) / three, (a.y + b.y + c.y) / three,
+                        (a.z + b.z + c.z) / three};
     }
-    dual3 ab2 = dvdot(ab, ab), ac2 = dvdot(ac, ac);
-    dvec t = dvec{ab2 * ac.x - ac2 * ab.x, ab2 * ac.y - ac2 * ab.y, ab2 * ac.z - ac2 * ab.z};
-    dvec cr = dvcross(t, n);
-    dual3 inv = dconst(1.0) / (dconst(2.0) * n2);
+    dualn<ND> ab2 = dvdot(ab, ab), ac2 = dvdot(ac, ac);
+    dvec<ND> t = dvec<ND>{ab2 * ac.x - ac2 * ab.x, ab2 * ac.y - ac2 * ab.y, ab2 * ac.z - ac2 * ab.z};
+    dvec<ND> cr = dvcross(t, n);
+    dualn<ND> inv = dconst<ND>(1.0) / (dconst<ND>(2.0) * n2);
     return dvadd(a, dvscale(cr, inv));
 }
 
-__device__ __forceinline__ dvec tet_cc_d(dvec a, dvec b, dvec c, dvec d) {
-    dvec ba = dvsub(b, a), ca = dvsub(c, a), da = dvsub(d, a);
-    dvec x1 = dvcross(ba, ca), x2 = dvcross(da, ba), x3 = dvcross(ca, da);
-    dvec m1 = dvscale(x1, dvdot(da, da));
-    dvec m2 = dvscale(x2, dvdot(ca, ca));
-    dvec m3 = dvscale(x3, dvdot(ba, ba));
-    dvec s = dvadd(m3, dvadd(m1, m2));
-    dual3 den = dconst(2.0) * dvdot(ba, x3);
+template <int ND>
+__device__ __forceinline__ dvec<ND> tet_cc_d(dvec<ND> a, dvec<ND> b, dvec<ND> c, dvec<ND> d) {
+    dvec<ND> ba = dvsub(b, a), ca = dvsub(c, a), da = dvsub(d, a);
+    dvec<ND> x1 = dvcross(ba, ca), x2 = dvcross(da, ba), x3 = dvcross(ca, da);
+    dvec<ND> m1 = dvscale(x1, dvdot(da, da));
+    dvec<ND> m2 = dvscale(x2, dvdot(ca, ca));
+    dvec<ND> m3 = dvscale(x3, dvdot(ba, ba));
+    dvec<ND> s = dvadd(m3, dvadd(m1, m2));
+    dualn<ND> den = dconst<ND>(2.0) * dvdot(ba, x3);
     if (fabs(den.v) < 1e-30) {
-        const dual3 q = dconst(0.25);
-        return dvec{(a.x + b.x + c.x + d.x) * q, (a.y + b.y + c.y + d.y) * q,
-                    (a.z + b.z + c.z + d.z) * q};
+        const dualn<ND> q = dconst<ND>(0.25);
+        return dvec<ND>{(a.x + b.x + c.x + d.x) * q, (a.y + b.y + c.y + d.y) * q,
+                        (a.z + b.z + c.z + d.z) * q};
     }
-    return dvadd(dvscale(s, dconst(1.0) / den), a);
+    return dvadd(dvscale(s, dconst<ND>(1.0) / den), a);
 }
 
-__device__ __forceinline__ dual3 subcell_volume_d(dvec pk, dvec pa, dvec pb, dvec pc, dvec ct,
-                                                  dvec fab, dvec fac, dvec fbc) {
-    dvec ta = dvsub(pa, pk), tb = dvsub(pb, pk), tc = dvsub(pc, pk);
-    dual3 sv = dvdot(ta, dvcross(tb, tc));
-    dvec a = pa, b = pb;
+template <int ND>
+__device__ __forceinline__ dualn<ND> subcell_volume_d(dvec<ND> pk, dvec<ND> pa, dvec<ND> pb, dvec<ND> pc,
+                                                      dvec<ND> ct, dvec<ND> fab, dvec<ND> fac,
+                                                      dvec<ND> fbc) {
+    dvec<ND> ta = dvsub(pa, pk), tb = dvsub(pb, pk), tc = dvsub(pc, pk);
+    dualn<ND> sv = dvdot(ta, dvcross(tb, tc));
+    dvec<ND> a = pa, b = pb;
     if (sv.v < 0) {
         a = pb;
         b = pa;
-        dvec t = fac;
+        dvec<ND> t = fac;
         fac = fbc;
         fbc = t;
     }
-    dvec df = dvsub(fab, pk), dg = dvsub(fac, pk), dh = dvsub(fbc, pk), dt = dvsub(ct, pk);
-    dvec c1 = dvcross(df, dt), c2 = dvcross(dt, dg), c3 = dvcross(dh, dt);
-    dvec e1 = dvsub(a, b), e2 = dvsub(a, pc), e3 = dvsub(b, pc);
-    dual3 vol = e1.x * c1.x;
+    dvec<ND> df = dvsub(fab, pk), dg = dvsub(fac, pk), dh = dvsub(fbc, pk), dt = dvsub(ct, pk);
+    dvec<ND> c1 = dvcross(df, dt), c2 = dvcross(dt, dg), c3 = dvcross(dh, dt);
+    dvec<ND> e1 = dvsub(a, b), e2 = dvsub(a, pc), e3 = dvsub(b, pc);
+    dualn<ND> vol = e1.x * c1.x;
     vol = vol + e1.y * c1.y;
     vol = vol + e1.z * c1.z;
     vol = vol + e2.x * c2.x;
@@ -113,7 +162,22 @@ __device__ __forceinline__ dual3 subcell_volume_d(dvec pk, dvec pa, dvec pb, dve
     vol = vol + e3.x * c3.x;
     vol = vol + e3.y * c3.y;
     vol = vol + e3.z * c3.z;
-    return vol / dconst(12.0);
+    return vol / dconst<ND>(12.0);
+}
+
+// the query as a dual vector with derivative seeds along x, y, z (ND = 3) or
+// along the one axis given (ND = 1)
+template <int ND>
+__device__ __forceinline__ dvec<ND> query_dual(dv3 q, int axis) {
+    dvec<ND> Q = dvconst<ND>(q);
+    if (ND == 3) {
+        Q.x.d[0] = 1.0;
+        Q.y.d[ND > 1 ? 1 : 0] = 1.0;
+        Q.z.d[ND > 2 ? 2 : 0] = 1.0;
+    } else {
+        (axis == 0 ? Q.x : (axis == 1 ? Q.y : Q.z)).d[0] = 1.0;
+    }
+    return Q;
 }
 
 // Gradient of sum_j c_j * (virtual-tet term of vertex j) over the three
@@ -122,28 +186,43 @@ __device__ __forceinline__ dual3 subcell_volume_d(dvec pk, dvec pa, dvec pb, dve
 // evaluates its two (vertex, query, vertex) triangle circumcentres in the
 // forward pass's own argument order (natural_insertionfree.c:708-714), so
 // its value part is bit-identical to the forward's.  One loop iteration per
-// term keeps the live dual state small (it would otherwise spill).
+// term keeps the live dual state small.  NIF_GRAD_ND = 1 differentiates one
+// axis per pass (three passes, a third of the live derivative state).
+#ifndef NIF_GRAD_ND
+#define NIF_GRAD_ND 3
+#endif
 __device__ __forceinline__ dv3 virtual_face_grad(dv3 q, dv3 fa, dv3 fb, dv3 fc, dv3 cface, double c0,
                                                  double c1, double c2) {
-    const dvec Q = dvec{dual3{q.x, 1.0, 0.0, 0.0}, dual3{q.y, 0.0, 1.0, 0.0}, dual3{q.z, 0.0, 0.0, 1.0}};
-    const dvec ct = tet_cc_d(Q, dvconst(fa), dvconst(fb), dvconst(fc));
-    dv3 gsum = dv3{0.0, 0.0, 0.0};
+    constexpr int ND = NIF_GRAD_ND;
+    double gx = 0.0, gy = 0.0, gz = 0.0;
 #pragma unroll 1
-    for (int j = 0; j < 3; j++) {
-        const double cj = j == 0 ? c0 : (j == 1 ? c1 : c2);
-        if (cj == 0.0) continue;
-        const dv3 k = j == 0 ? fa : (j == 1 ? fb : fc);
-        const dv3 n = j == 0 ? fb : (j == 1 ? fc : fa);  // face_verts[(j+1)%3]
-        const dv3 p = j == 0 ? fc : (j == 1 ? fa : fb);  // face_verts[(j+2)%3]
-        const dvec K = dvconst(k), N = dvconst(n), P = dvconst(p);
-        const dvec t1 = tri_cc_d(K, Q, N);
-        const dvec t2 = tri_cc_d(K, Q, P);
-        const dual3 v = subcell_volume_d(K, Q, N, P, ct, t1, t2, dvconst(cface));
-        gsum.x += cj * v.dx;
-        gsum.y += cj * v.dy;
-        gsum.z += cj * v.dz;
+    for (int axis = 0; axis < 3; axis += ND) {
+        const dvec<ND> Q = query_dual<ND>(q, axis);
+        const dvec<ND> ct = tet_cc_d<ND>(Q, dvconst<ND>(fa), dvconst<ND>(fb), dvconst<ND>(fc));
+#pragma unroll 1
+        for (int j = 0; j < 3; j++) {
+            const double cj = j == 0 ? c0 : (j == 1 ? c1 : c2);
+            if (cj == 0.0) continue;
+            const dv3 k = j == 0 ? fa : (j == 1 ? fb : fc);
+            const dv3 n = j == 0 ? fb : (j == 1 ? fc : fa);  // face_verts[(j+1)%3]
+            const dv3 p = j == 0 ? fc : (j == 1 ? fa : fb);  // face_verts[(j+2)%3]
+            const dvec<ND> K = dvconst<ND>(k), N = dvconst<ND>(n), P = dvconst<ND>(p);
+            const dvec<ND> t1 = tri_cc_d<ND>(K, Q, N);
+            const dvec<ND> t2 = tri_cc_d<ND>(K, Q, P);
+            const dualn<ND> v = subcell_volume_d<ND>(K, Q, N, P, ct, t1, t2, dvconst<ND>(cface));
+            if (ND == 3) {
+                gx += cj * v.d[0];
+                gy += cj * v.d[ND > 1 ? 1 : 0];
+                gz += cj * v.d[ND > 2 ? 2 : 0];
+            } else {
+                const double t = cj * v.d[0];
+                gx += axis == 0 ? t : 0.0;
+                gy += axis == 1 ? t : 0.0;
+                gz += axis == 2 ? t : 0.0;
+            }
+        }
     }
-    return gsum;
+    return dv3{gx, gy, gz};
 }
 
 }  // namespace nif

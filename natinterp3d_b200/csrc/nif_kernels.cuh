@@ -4,7 +4,8 @@
 // Per query (natinterp3d's getWeightsSingleQueryIF, natural_insertionfree.c:591-738):
 //   1. locate   seed tet = the tet whose centroid is nearest to the query, as
 //               natinterp3d's k-d tree returns it (delaunay.c:392-395), found in
-//               an octree over the Morton-sorted centroids; then
+//               a uniform grid of centroids (an octree where the grid is too
+//               coarse); then
 //               natinterp3d's visibility walk (delaunay.c:398-405), the four
 //               face tests of a step on 4 lanes
 //   2. cavity   the connected set of tets whose circumsphere strictly contains
@@ -97,8 +98,17 @@ struct MeshView {
     int n;                             // data vertices (ids >= n are super-simplex vertices)
     int nv, nt;
     int pmode;                         // PRED_*
-    int gdim[3];                       // query bucketing: cell of x along axis a is
-    double glo[3], ginv[3];            // (x - glo) * ginv / gdim of the data bounding box
+    // Uniform grid over the data bounding box, gdim cells per axis (cell of x
+    // along axis a: floor((x - glo) * ginv), clamped), about two centroids a
+    // cell: the centroids of cell k are gitems[gstart[k] .. gstart[k + 1]),
+    // x, y, z and the tet id (as a double), in no particular order.  The
+    // seed search reads it first; query bucketing normalises by the same box.
+    const int *__restrict__ gstart;
+    const d4 *__restrict__ gitems;
+    int gdim[3];
+    double glo[3], ginv[3];
+    double gh[3];                      // cell size, 1 / ginv
+    double gext;                       // largest extent of the grid (margins)
 };
 
 __device__ __forceinline__ int comp(const int4 &v, int i) {
@@ -355,6 +365,90 @@ __device__ int nearest_centroid(const MeshView &M, const dv3 q, const Grp<G> &g,
     return bid == INT_MAX ? 0 : bid;
 }
 
+constexpr int GRID_DENSE = 256;  // centroids in a search block beyond which the octree searches
+constexpr int GRID_RMAX = 3;     // largest block radius (cells) the grid search widens to
+
+// The nearest tet centroid to q (same distance and ties as nearest_centroid)
+// from the uniform grid: the centroids of the cells within Chebyshev radius
+// r of q's cell, one lane per cell, r = 1 first; done once the best distance
+// is below the distance from q to the searched block's open sides (sides on
+// the grid's boundary are closed: centroids beyond them are clamped into the
+// boundary cells, which have been searched).  Returns -1 where the block
+// holds more than GRID_DENSE centroids or r would exceed GRID_RMAX: the
+// octree search takes over there (clustered data, far-away queries).
+template <int G>
+__device__ int grid_nearest(const MeshView &M, const dv3 q) {
+    static_assert(G == 32, "one lane per cell of a 3x3x3 block");
+    const double c[3] = {q.x, q.y, q.z};
+    double f[3];  // q's position in cell units
+    int ic[3];
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        f[a] = (c[a] - M.glo[a]) * M.ginv[a];
+        ic[a] = f[a] > 0.0 ? (f[a] < (double)(M.gdim[a] - 1) ? (int)f[a] : M.gdim[a] - 1) : 0;
+    }
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    double best = INFINITY;
+    int bid = INT_MAX;
+    for (int r = 1; r <= GRID_RMAX; r++) {
+        const int w = 2 * r + 1, ncell = w * w * w;
+        // this round's cells: the 27 of the 3x3x3 block, then the shell at
+        // Chebyshev radius r
+        int total = 0;
+        for (int k0 = 0; k0 < ncell; k0 += 32) {
+            const int k = k0 + lane;
+            int a = 0, b = 0;
+            int dx, dy, dz;
+            bool take;
+            if (r == 1) {
+                dx = lane % 3 - 1, dy = (lane / 3) % 3 - 1, dz = lane / 9 - 1;
+                take = lane < 27;
+            } else {
+                dx = k % w - r, dy = (k / w) % w - r, dz = k / (w * w) - r;
+                take = k < ncell && max(abs(dx), max(abs(dy), abs(dz))) == r;
+            }
+            const int x = ic[0] + dx, y = ic[1] + dy, z = ic[2] + dz;
+            if (take && x >= 0 && y >= 0 && z >= 0 && x < M.gdim[0] && y < M.gdim[1] && z < M.gdim[2]) {
+                const int cell = (z * M.gdim[1] + y) * M.gdim[0] + x;
+                a = M.gstart[cell];
+                b = M.gstart[cell + 1];
+            }
+            total += __reduce_add_sync(full, b - a);
+            if (total > GRID_DENSE) return -1;
+            for (int i = a; i < b; i++) {
+                const d4 e = M.gitems[i];
+                const double d = kd_dist2(e, q);
+                const int id = (int)e.w;
+                if (d < best || (d == best && id < bid)) {
+                    best = d;
+                    bid = id;
+                }
+            }
+        }
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+            const double od = __shfl_xor_sync(full, best, off);
+            const int oi = __shfl_xor_sync(full, bid, off);
+            if (od < best || (od == best && oi < bid)) {
+                best = od;
+                bid = oi;
+            }
+        }
+        // distance from q to the block's open sides (not on the grid's boundary)
+        double lb = INFINITY;
+#pragma unroll
+        for (int a = 0; a < 3; a++) {
+            if (ic[a] - r > 0) lb = fmin(lb, (f[a] - (double)(ic[a] - r)) * M.gh[a]);
+            if (ic[a] + r < M.gdim[a] - 1) lb = fmin(lb, ((double)(ic[a] + r + 1) - f[a]) * M.gh[a]);
+        }
+        if (lb == INFINITY) return bid == INT_MAX ? -1 : bid;  // the block covers the grid
+        const double m = lb - 1e-9 * M.gext;
+        if (bid != INT_MAX && m > 0.0 && best < m * m * (1.0 - 1e-12)) return bid;
+    }
+    return -1;
+}
+
 // Per-group scratch.  The first union member is live during the cavity
 // search, the second only during the single-lane replay of natinterp3d's
 // visiting order.  Index types are the narrowest that hold each capacity.
@@ -563,30 +657,23 @@ __device__ __forceinline__ int neighbour_slot(const W &ws, int v) {
     return s >= 0 ? ws.vh_slot[s] : -1;
 }
 
-// The Sibson row of centred query q.  On ST_OK the row is ws.nbr_vid[0..nnb)
-// with normalised weights ws.acc[0..nnb), in natinterp3d's column order.
-// With FULL = false only the combinatorial part is built (cavity, visiting
-// order, boundary faces, neighbours in column order) and no volume is
-// computed; the query-gradient kernel needs nothing more.  PM selects the
-// predicate variant (PM_*); PM_RESOLVE needs xs, NIF_EXACT_SCRATCH doubles of
-// global scratch owned by this group.
-template <int G, class W, bool FULL = true, int PM = PM_PLAIN>
-__device__ RowInfo sibson_row(const MeshView &M, const dv3 q, W &ws, const Grp<G> &g,
-                              double *xs = nullptr) {
-    using cav_t = typename W::cav_t;
-    using slot_t = typename W::slot_t;
-    RowInfo r{ST_OK, 0, 0, false, false, 0.0, 0, 0, 0, 0, 0};
-    // filters run only for the non-default modes
+// Point location (natinterp3d's findContainingSimplex, delaunay.c:383-407):
+// the seed is the nearest tet centroid, then natinterp3d's visibility walk.
+// Returns the located tet; r.status / r.outside report a walk that hit its
+// step limit or left the super-simplex, r.steps counts the steps.  scratch:
+// 64 ints of group scratch (the octree search's).  PM selects the predicate
+// variant as in sibson_row; *on_face is set in PM_RESOLVE / PRED_EXACT when a
+// face test of the located tet is exactly zero.
+template <int G, int PM>
+__device__ int locate(const MeshView &M, const dv3 q, const Grp<G> &g, int *scratch, RowInfo &r,
+                      bool &on_face, double *xs = nullptr) {
     const bool filt = PM != PM_PLAIN && M.pmode != PRED_FAST;
-    bool on_face = false;  // PRED_EXACT: a face test of the located tet is exactly zero
-
-    // ---- 1. point location -------------------------------------------------
-    // seed: the nearest tet centroid, then natinterp3d's walk
-    int t = nearest_centroid<G>(M, q, g, reinterpret_cast<int *>(ws.acc));
+    int t = grid_nearest<G>(M, q);
+    if (t < 0) t = nearest_centroid<G>(M, q, g, scratch);
     for (;;) {
         if (r.steps >= WALK_LIMIT) {
             r.status = ST_WALK;
-            return r;
+            return t;
         }
         ++r.steps;
         const int4 p = M.tv[t];
@@ -613,7 +700,7 @@ __device__ RowInfo sibson_row(const MeshView &M, const dv3 q, W &ws, const Grp<G
             const int fn = m ? __ffs(m) - 1 : 4;
             if (g.ballot(unc) & ((2u << fn) - 1u)) {
                 r.status = ST_UNCERTAIN;
-                return r;
+                return t;
             }
         } else {
             if (filt) {
@@ -628,13 +715,41 @@ __device__ RowInfo sibson_row(const MeshView &M, const dv3 q, W &ws, const Grp<G
                 m = g.ballot(sg < 0);
             }
         }
-        if (!m) break;
+        if (!m) return t;
         const int nb = comp(nbs, __ffs(m) - 1);
         if (nb < 0) {
             r.outside = true;
-            return r;
+            return t;
         }
         t = nb;
+    }
+}
+
+// The Sibson row of centred query q.  On ST_OK the row is ws.nbr_vid[0..nnb)
+// with normalised weights ws.acc[0..nnb), in natinterp3d's column order.
+// With FULL = false only the combinatorial part is built (cavity, visiting
+// order, boundary faces, neighbours in column order) and no volume is
+// computed; the query-gradient kernel needs nothing more.  PM selects the
+// predicate variant (PM_*); PM_RESOLVE needs xs, NIF_EXACT_SCRATCH doubles of
+// global scratch owned by this group.  With LOC the query was located by
+// k_locate (PM_PLAIN only): `located` is its tet, and this code holds no
+// point location of its own.
+template <int G, class W, bool FULL = true, int PM = PM_PLAIN, bool LOC = false>
+__device__ RowInfo sibson_row(const MeshView &M, const dv3 q, W &ws, const Grp<G> &g,
+                              double *xs = nullptr, int located = 0) {
+    static_assert(!LOC || PM == PM_PLAIN, "located rows use natinterp3d's signs");
+    using cav_t = typename W::cav_t;
+    using slot_t = typename W::slot_t;
+    RowInfo r{ST_OK, 0, 0, false, false, 0.0, 0, 0, 0, 0, 0};
+    // filters run only for the non-default modes
+    const bool filt = PM != PM_PLAIN && M.pmode != PRED_FAST;
+    bool on_face = false;  // PRED_EXACT: a face test of the located tet is exactly zero
+
+    // ---- 1. point location -------------------------------------------------
+    int t = located;
+    if constexpr (!LOC) {
+        t = locate<G, PM>(M, q, g, reinterpret_cast<int *>(ws.acc), r, on_face, xs);
+        if (r.status != ST_OK || r.outside) return r;
     }
     const int start = t;
 
