@@ -340,10 +340,6 @@ def _weights_leg(interp, queries, steps, warmup, cpu, sample_n, workload):
     lib.nif_profile_enable(0)
     nnz = int(summ['nnz'])
     del rowptr, cols, vals
-    # the CSR epilogue (row-pointer scan, then the staged rows copied into the
-    # final arrays): HBM-bound, compulsory bytes = staged rows read (4 + 8 B an
-    # entry) + final CSR written (4 + 8 B an entry) + row counts / offsets
-    epi_bytes = nnz * 24 + M * 20
     e2e = []
     for _ in range(2):
         torch.cuda.synchronize()
@@ -352,9 +348,9 @@ def _weights_leg(interp, queries, steps, warmup, cpu, sample_n, workload):
         e2e.append(time.perf_counter() - t0)
     out = {'value': M / (ms * 1e-3), 'unit': 'queries/s', 'ms_per_step': ms, 'steps': steps,
            'warmup': warmup, 'nnz': nnz,
-           'phase_ms': {'bucketing': ph[0], 'rows_fast': ph[1], 'rows_large': ph[2],
-                        'csr_epilogue': ph[3]},
-           'csr_epilogue_gbs': epi_bytes / (ph[3] * 1e-3) / 1e9 if ph[3] > 0 else None,
+           # count call's phases (the fill call's compaction is not among them)
+           'phase_ms': {'bucketing': ph[0], 'rows': ph[1], 'rows_large': ph[2],
+                        'row_pointer_scan': ph[3]},
            'e2e': {'value': M / e2e[-1], 'unit': 'queries/s', 'h2d_bytes_per_step': int(queries.nbytes),
                    'd2h_bytes_per_step': int(W.data.nbytes + W.indices.nbytes + W.indptr.nbytes)},
            'config': {'workload': workload}}

@@ -56,6 +56,25 @@ using FastWS = Workspace<256, 96, 128, 64, 128, FAST_G, uint8_t, int8_t>;
 constexpr int LARGE_G = 32;
 using LargeWS = Workspace<16384, 4096, 8192, 2048, 8192, LARGE_G, uint16_t, int16_t>;
 constexpr int ROW_STAGE = 24;         // get_weights: entries staged per row (mean about 15.5)
+using CavWS = CavWorkspace<256, 96, FAST_G, uint8_t, int8_t>;
+using VolWS = VolWorkspace<REC_CAV, 128, 64, 128, FAST_G>;
+// rows a record buffer holds: calls run in chunks of these (measured: 256k-
+// and 64k-row chunks, whose records stay in L2, ran 6 % and 25 % slower on
+// 10M queries -- the launches' tails cost more than the DRAM round trip)
+#ifndef NIF_REC_CHUNK
+#define NIF_REC_CHUNK (1 << 20)
+#endif
+constexpr int REC_CHUNK = NIF_REC_CHUNK;
+// resident blocks per SM of the split kernels (0: the mesh's blocks_per_sm).
+// The cavity kernel is issue-bound and fits 10 blocks in 48 registers (1-2 %
+// faster than 8 on 10M queries); the volume kernel spills at 10 (16 % slower)
+// and follows the mesh's setting.
+#ifndef NIF_CAV_OCC
+#define NIF_CAV_OCC 10
+#endif
+#ifndef NIF_VOL_OCC
+#define NIF_VOL_OCC 0
+#endif
 
 constexpr int FAST_BLOCK = 128;       // 4 warps
 constexpr int LARGE_GROUPS = 64;      // concurrent large-row groups (one warp each)
@@ -76,6 +95,7 @@ struct DevSummary {
     int first_status;
     int large_count;  // rows queued for the large kernel
     int refill_count; // get_weights: fast-kernel rows longer than ROW_STAGE
+    int wide_count;   // split rows whose cavity exceeds a record (the fused kernel takes them)
     // predicate evaluations the filter could not certify / whose decision the
     // exact sign changes (PRED_AUDIT and PRED_EXACT meshes)
     unsigned long long orient_unc, orient_flip, insphere_unc, insphere_flip;
@@ -734,7 +754,20 @@ __global__ void k_spmm(int64_t M, int D, const int32_t *__restrict__ rowptr,
         const int64_t i = u / D;
         const int d = (int)(u - i * D);
         CT acc = (CT)0;
-        for (int e = rowptr[i]; e < rowptr[i + 1]; e++)
+        int e = rowptr[i];
+        const int e1 = rowptr[i + 1];
+        // four entries' loads issued together; the sum stays in stored order
+        for (; e + 4 <= e1; e += 4) {
+            const int c0 = cols[e], c1 = cols[e + 1], c2 = cols[e + 2], c3 = cols[e + 3];
+            const CT w0 = (CT)vals[e], w1 = (CT)vals[e + 1], w2 = (CT)vals[e + 2], w3 = (CT)vals[e + 3];
+            const CT x0 = (CT)x[(int64_t)c0 * D + d], x1 = (CT)x[(int64_t)c1 * D + d];
+            const CT x2 = (CT)x[(int64_t)c2 * D + d], x3 = (CT)x[(int64_t)c3 * D + d];
+            acc = Arith<CT>::add(acc, Arith<CT>::mul(w0, x0));
+            acc = Arith<CT>::add(acc, Arith<CT>::mul(w1, x1));
+            acc = Arith<CT>::add(acc, Arith<CT>::mul(w2, x2));
+            acc = Arith<CT>::add(acc, Arith<CT>::mul(w3, x3));
+        }
+        for (; e < e1; e++)
             acc = Arith<CT>::add(acc, Arith<CT>::mul((CT)vals[e], (CT)x[(int64_t)cols[e] * D + d]));
         y[u] = acc;
     }
@@ -874,7 +907,21 @@ __global__ void k_spmm_t(int64_t N, int D, const int32_t *__restrict__ colptr,
         const int64_t k = u / D;
         const int d = (int)(u - k * D);
         CT acc = (CT)0;
-        for (int p = colptr[k]; p < colptr[k + 1]; p++) {
+        int p = colptr[k];
+        const int p1 = colptr[k + 1];
+        // four entries' loads issued together; the sum stays in ascending row order
+        for (; p + 4 <= p1; p += 4) {
+            const int e0 = perm[p], e1 = perm[p + 1], e2 = perm[p + 2], e3 = perm[p + 3];
+            const int r0 = rowof[e0], r1 = rowof[e1], r2 = rowof[e2], r3 = rowof[e3];
+            const CT w0 = (CT)vals[e0], w1 = (CT)vals[e1], w2 = (CT)vals[e2], w3 = (CT)vals[e3];
+            const CT x0 = (CT)x[(int64_t)r0 * D + d], x1 = (CT)x[(int64_t)r1 * D + d];
+            const CT x2 = (CT)x[(int64_t)r2 * D + d], x3 = (CT)x[(int64_t)r3 * D + d];
+            acc = Arith<CT>::add(acc, Arith<CT>::mul(w0, x0));
+            acc = Arith<CT>::add(acc, Arith<CT>::mul(w1, x1));
+            acc = Arith<CT>::add(acc, Arith<CT>::mul(w2, x2));
+            acc = Arith<CT>::add(acc, Arith<CT>::mul(w3, x3));
+        }
+        for (; p < p1; p++) {
             const int e = perm[p];
             acc = Arith<CT>::add(acc, Arith<CT>::mul((CT)vals[e], (CT)x[(int64_t)rowof[e] * D + d]));
         }
@@ -885,6 +932,66 @@ __global__ void k_spmm_t(int64_t N, int D, const int32_t *__restrict__ colptr,
 // ---------------------------------------------------------------------------
 // row kernels
 // ---------------------------------------------------------------------------
+// problem of row i in a batch: off[p] <= i < off[p + 1]
+__device__ __forceinline__ int find_problem(const int64_t *__restrict__ off, int P, int64_t i) {
+    int lo = 0, hi = P;  // off[lo] <= i < off[hi]
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (off[mid] <= i) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+
+// Where the split row kernels find a row's mesh and key centroid.
+// OneMesh: every row queries one mesh (passed as a __grid_constant__ kernel
+// argument).  ManyMeshes: a batch; row i belongs to problem p with
+// qoff[p] <= i < qoff[p + 1], whose view the group caches in `slot` while
+// consecutive rows stay in the same problem (`cur`).
+struct OneMesh {
+    MeshView M;
+    Centroid cen;
+    __device__ __forceinline__ const MeshView &get(int64_t, int &, MeshView *, const Grp<FAST_G> &,
+                                                   const double *&c) const {
+        c = cen.c;
+        return M;
+    }
+};
+
+struct ManyMeshes {
+    const MeshView *__restrict__ views;
+    const int64_t *__restrict__ qoff;
+    int P;
+    const double *__restrict__ cens;
+    __device__ __forceinline__ const MeshView &get(int64_t i, int &cur, MeshView *slot,
+                                                   const Grp<FAST_G> &g, const double *&c) const {
+        const int p = find_problem(qoff, P, i);
+        if (p != cur) {
+            g.sync();
+            if (g.lane == 0) *slot = views[p];
+            g.sync();
+            cur = p;
+        }
+        c = cens + 3 * p;
+        return *slot;
+    }
+};
+
+// Rows [s, s1) of work item t of the tiled schedule: tiles of `tile` rows,
+// then the last `tail` rows (about `tile` per resident group) one at a
+// time, so that the groups finish together instead of waiting on the last
+// full tiles.
+__device__ __forceinline__ void tile_range(unsigned long long t, int tile, int64_t nrows, int64_t tail,
+                                           int64_t &s, int64_t &s1) {
+    const int64_t nhead = nrows > tail ? (nrows - tail) / tile : 0;
+    if ((int64_t)t < nhead) {
+        s = (int64_t)t * tile;
+        s1 = s + tile;
+    } else {
+        s = nhead * tile + ((int64_t)t - nhead);
+        s1 = min(nrows, s + 1);
+    }
+}
+
 struct LargeQueue {
     int *__restrict__ list;  // [M]
 };
@@ -899,14 +1006,10 @@ __device__ __forceinline__ void record(DevSummary *sum, const RowInfo &r, int la
 // PM_FILTER; OCC resident blocks per SM.  With tile == 0 group k takes rows
 // k, k + ng, k + 2 ng, ...; with tile > 0 it takes tiles of `tile`
 // consecutive rows from the device counter (zeroed before the launch).
-// With LOC the rows were located by k_locate: located[i] is row i's tet, -1
-// outside the super-simplex, -2 a walk that hit its step limit; the kernel
-// then holds no point-location code (a smaller instruction footprint).
-template <class QT, class Sink, int PM, int OCC, bool LOC>
+template <class QT, class Sink, int PM, int OCC>
 __global__ void __launch_bounds__(FAST_BLOCK, OCC) k_rows_fast(MeshView M, const QT *__restrict__ Q,
                                                           Centroid cen, const int *__restrict__ order,
                                                           int64_t nrows, const int *nrows_dev,
-                                                          const int *__restrict__ located,
                                                           Sink sink, LargeQueue lq,
                                                           DevSummary *sum, int tile,
                                                           unsigned long long *counter) {
@@ -928,23 +1031,12 @@ __global__ void __launch_bounds__(FAST_BLOCK, OCC) k_rows_fast(MeshView M, const
             unsigned long long t = 0;
             if (g.lane == 0) t = atomicAdd(counter, 1ull);
             t = __shfl_sync(g.mask, t, 0, G);
-            s = (int64_t)t * tile;
+            tile_range(t, tile, nrows, ng * tile, s, s1);
             if (s >= nrows) break;
-            s1 = min(nrows, s + (int64_t)tile);
         }
         const int64_t i = order[s];
         const dv3 q = load_query(Q, i, cen.c);
-        RowInfo r;
-        if constexpr (LOC) {
-            const int t = located[i];
-            if (t >= 0) {
-                r = sibson_row<G, FastWS, Sink::FULL, PM, true>(M, q, ws, g, nullptr, t);
-            } else {
-                r = RowInfo{t == -2 ? ST_WALK : ST_OK, 0, 0, t == -1, false, 0.0, 0, 0, 0, 0, 0};
-            }
-        } else {
-            r = sibson_row<G, FastWS, Sink::FULL, PM>(M, q, ws, g);
-        }
+        const RowInfo r = sibson_row<G, FastWS, Sink::FULL, PM>(M, q, ws, g);
         steps += r.steps;
         if (r.status == ST_CAPACITY || r.status == ST_UNCERTAIN) {
             if (g.lane == 0) {
@@ -966,18 +1058,21 @@ __global__ void __launch_bounds__(FAST_BLOCK, OCC) k_rows_fast(MeshView M, const
 }
 
 // Point location of every row (natinterp3d's signs): one warp per row, rows
-// in bucket order as k_rows_fast takes them; located[i] = the tet, -1
+// in bucket order as the row kernels take them; located[i] = the tet, -1
 // outside the super-simplex, -2 a walk that hit its step limit.
-template <class QT>
-__global__ void __launch_bounds__(FAST_BLOCK) k_locate(MeshView M, const QT *__restrict__ Q, Centroid cen,
+template <class QT, class Rows>
+__global__ void __launch_bounds__(FAST_BLOCK) k_locate(const __grid_constant__ Rows rows,
+                                                       const QT *__restrict__ Q,
                                                        const int *__restrict__ order, int64_t nrows,
                                                        int *__restrict__ located, DevSummary *sum,
                                                        int tile, unsigned long long *counter) {
     constexpr int G = 32;
     constexpr int GPB = FAST_BLOCK / G;
     __shared__ int scratch[GPB][64];
+    __shared__ MeshView sview[GPB];
     Grp<G> g;
     int *scr = scratch[threadIdx.x / G];
+    int cur = -1;
     const int64_t gid = tile <= 0 ? (int64_t)blockIdx.x * GPB + threadIdx.x / G : 0;
     const int64_t ng = (int64_t)gridDim.x * GPB;
     unsigned long long steps = 0;
@@ -988,12 +1083,13 @@ __global__ void __launch_bounds__(FAST_BLOCK) k_locate(MeshView M, const QT *__r
             unsigned long long t = 0;
             if (g.lane == 0) t = atomicAdd(counter, 1ull);
             t = __shfl_sync(g.mask, t, 0, G);
-            s = (int64_t)t * tile;
+            tile_range(t, tile, nrows, ng * tile, s, s1);
             if (s >= nrows) break;
-            s1 = min(nrows, s + (int64_t)tile);
         }
         const int64_t i = order[s];
-        const dv3 q = load_query(Q, i, cen.c);
+        const double *cen;
+        const MeshView &M = rows.get(i, cur, &sview[threadIdx.x / G], g, cen);
+        const dv3 q = load_query(Q, i, cen);
         RowInfo r{ST_OK, 0, 0, false, false, 0.0, 0, 0, 0, 0, 0};
         bool on_face = false;
         const int t = locate<G, PM_PLAIN>(M, q, g, scr, r, on_face);
@@ -1003,6 +1099,115 @@ __global__ void __launch_bounds__(FAST_BLOCK) k_locate(MeshView M, const QT *__r
         s += tile <= 0 ? ng : 1;
     }
     if (g.lane == 0 && steps) atomicAdd(&sum->walk_steps, steps);
+}
+
+// The split row kernels (natinterp3d's signs, located rows): k_rows_cavity
+// writes each row's record, k_rows_volume reads it and emits the row.  Rows
+// are positions [0, nrows) of `order` (one chunk of a call); record s
+// belongs to position s.  Each kernel holds one half of the row code.
+// Rows whose cavity fits the shared-memory capacities but not a record are
+// queued in `wide` for the fused row kernel, larger ones for the large kernel.
+template <class QT, class Rows, int OCC>
+__global__ void __launch_bounds__(FAST_BLOCK, OCC)
+    k_rows_cavity(const __grid_constant__ Rows rows, const QT *__restrict__ Q,
+                  const int *__restrict__ order, int64_t nrows, const int *__restrict__ located,
+                  RowHead *__restrict__ heads, RowEntry *__restrict__ ents, int *__restrict__ wide,
+                  LargeQueue lq, DevSummary *sum, int tile, unsigned long long *counter) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    constexpr int G = FAST_G;
+    constexpr int GPB = FAST_BLOCK / G;
+    __shared__ MeshView sview[GPB];
+    Grp<G> g;
+    CavWS &ws = reinterpret_cast<CavWS *>(smem)[threadIdx.x / G];
+    int cur = -1;
+    const int64_t gid = tile <= 0 ? (int64_t)blockIdx.x * GPB + threadIdx.x / G : 0;
+    const int64_t ng = (int64_t)gridDim.x * GPB;
+    int64_t s = gid, s1 = tile <= 0 ? nrows : 0;
+    for (;;) {
+        if (s >= s1) {
+            if (tile <= 0) break;
+            unsigned long long t = 0;
+            if (g.lane == 0) t = atomicAdd(counter, 1ull);
+            t = __shfl_sync(g.mask, t, 0, G);
+            tile_range(t, tile, nrows, ng * tile, s, s1);
+            if (s >= nrows) break;
+        }
+        const int64_t i = order[s];
+        const int t = located[i];
+        RowHead h{0, t, RS_OK, 0};
+        if (t == -1) {
+            h.state = RS_OUTSIDE;
+        } else if (t < 0) {
+            h.state = RS_WALK;
+        } else {
+            const double *cen;
+            const MeshView &M = rows.get(i, cur, &sview[threadIdx.x / G], g, cen);
+            const dv3 q = load_query(Q, i, cen);
+            const int rc = cavity_record<G>(M, q, ws, g, t, h, ents + s * REC_CAV);
+            if (rc != REC_DONE) {
+                h.state = RS_QUEUED;
+                if (g.lane == 0) {
+                    if (rc == REC_WIDE)
+                        wide[atomicAdd(&sum->wide_count, 1)] = (int)i;
+                    else
+                        lq.list[atomicAdd(&sum->large_count, 1)] = (int)i;
+                }
+            }
+        }
+        if (g.lane == 0) heads[s] = h;
+        g.sync();
+        s += tile <= 0 ? ng : 1;
+    }
+}
+
+template <class QT, class Rows, class Sink, int OCC>
+__global__ void __launch_bounds__(FAST_BLOCK, OCC)
+    k_rows_volume(const __grid_constant__ Rows rows, const QT *__restrict__ Q,
+                  const int *__restrict__ order, int64_t nrows, const RowHead *__restrict__ heads,
+                  const RowEntry *__restrict__ ents, Sink sink, LargeQueue lq, DevSummary *sum,
+                  int tile, unsigned long long *counter) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    constexpr int G = FAST_G;
+    constexpr int GPB = FAST_BLOCK / G;
+    __shared__ MeshView sview[GPB];
+    Grp<G> g;
+    VolWS &ws = reinterpret_cast<VolWS *>(smem)[threadIdx.x / G];
+    int cur = -1;
+    const int64_t gid = tile <= 0 ? (int64_t)blockIdx.x * GPB + threadIdx.x / G : 0;
+    const int64_t ng = (int64_t)gridDim.x * GPB;
+    int64_t s = gid, s1 = tile <= 0 ? nrows : 0;
+    for (;;) {
+        if (s >= s1) {
+            if (tile <= 0) break;
+            unsigned long long t = 0;
+            if (g.lane == 0) t = atomicAdd(counter, 1ull);
+            t = __shfl_sync(g.mask, t, 0, G);
+            tile_range(t, tile, nrows, ng * tile, s, s1);
+            if (s >= nrows) break;
+        }
+        const int64_t i = order[s];
+        const RowHead h = heads[s];
+        if (h.state != RS_QUEUED) {
+            const double *cen;
+            const MeshView &M = rows.get(i, cur, &sview[threadIdx.x / G], g, cen);
+            const dv3 q = load_query(Q, i, cen);
+            RowInfo r{ST_OK, 0, 0, h.state == RS_OUTSIDE, false, 0.0, 0, 0, 0, 0, 0};
+            if (h.state == RS_OK) r = volume_row<G, VolWS, Sink::FULL>(M, q, ws, g, h, ents + s * REC_CAV);
+            if (h.state == RS_WALK) r.status = ST_WALK;
+            if (r.status == ST_CAPACITY) {
+                if (g.lane == 0) lq.list[atomicAdd(&sum->large_count, 1)] = (int)i;
+            } else {
+                if (r.status != ST_OK && g.lane == 0) {
+                    atomicAdd(&sum->rows_failed, 1ull);
+                    atomicCAS(&sum->first_status, 0, NIF_ERR_WALK);
+                }
+                record<G>(sum, r, g.lane);
+                sink.template emit<G>(i, r.status == ST_OK ? r.nnb : 0, ws, g, false, M, q, r);
+            }
+        }
+        g.sync();
+        s += tile <= 0 ? ng : 1;
+    }
 }
 
 template <int G>
@@ -1250,6 +1455,9 @@ struct QueryLayout {
     LargeWS *large_ws;
     double *exact;          // NIF_EXACT_SCRATCH doubles per large-row group
     int *located;           // k_locate's tet per row (null: the row kernel locates)
+    RowHead *heads;         // split-row records of one chunk of rows
+    RowEntry *ents;
+    int *wide;              // split rows whose cavity exceeds a record
     // weights mode only
     int *cnt;
     uint8_t *staged;
@@ -1286,6 +1494,12 @@ QueryLayout carve_query(Carve &c, int64_t M, int mode) {
     L.large_ws = c.take<LargeWS>(LARGE_GROUPS);
     L.exact = c.take<double>((size_t)LARGE_GROUPS * NIF_EXACT_SCRATCH);
     L.located = c.take<int>(M > 0 ? M : 1);
+    {
+        const int64_t ch = M < REC_CHUNK ? (M > 0 ? M : 1) : REC_CHUNK;
+        L.heads = c.take<RowHead>(ch);
+        L.ents = c.take<RowEntry>(ch * REC_CAV);
+        L.wide = c.take<int>(M > 0 ? M : 1);
+    }
     if (mode == NIF_MODE_WEIGHTS) {
         const int64_t m1 = M > 0 ? M : 1;
         L.cnt = c.take<int>(m1);
@@ -1414,12 +1628,12 @@ inline int fit_tile(int tile, int64_t M, int per_sm, int num_sms, int gpb) {
 }
 
 // persistent grid of the fast row kernel: resident blocks per SM x SMs
-template <class QT, class Sink, int PM, int OCC, bool LOC>
+template <class QT, class Sink, int PM, int OCC>
 void launch_fast_occ(const nif_dmesh *m, const QT *Q, int64_t M, const Centroid &cen,
                      const RowSet &R, const Sink &sink, cudaStream_t st) {
     constexpr int GPB = FAST_BLOCK / FAST_G;
     const size_t smem = GPB * sizeof(FastWS);
-    auto kern = k_rows_fast<QT, Sink, PM, OCC, LOC>;
+    auto kern = k_rows_fast<QT, Sink, PM, OCC>;
     const int per_sm = resident_blocks(kern, FAST_BLOCK, smem);
     // tile is an upper bound: a call too small to give every resident group
     // two tiles takes smaller ones (or the static stride), so that small
@@ -1431,56 +1645,103 @@ void launch_fast_occ(const nif_dmesh *m, const QT *Q, int64_t M, const Centroid 
     if (blocks > cap) blocks = cap;
     if (blocks < 1) blocks = 1;
     if (tile > 0) cudaMemsetAsync(R.counter, 0, sizeof(unsigned long long), st);
-    kern<<<(unsigned)blocks, FAST_BLOCK, smem, st>>>(m->view, Q, cen, R.order, M, R.nrows_dev,
-                                                    R.located, sink, LargeQueue{R.large}, R.sum, tile,
-                                                    R.counter);
-}
-
-// k_locate over the rows of R (all of them: located rows are never a queue)
-template <class QT>
-void launch_locate(const nif_dmesh *m, const QT *Q, int64_t M, const Centroid &cen, const RowSet &R,
-                   int *located, cudaStream_t st) {
-    constexpr int GPB = FAST_BLOCK / 32;
-    auto kern = k_locate<QT>;
-    const int per_sm = resident_blocks(kern, FAST_BLOCK, 0);
-    const int tile = fit_tile(m->tune.tile, M, per_sm, m->num_sms, GPB);
-    int64_t blocks = (M + GPB - 1) / GPB;
-    if (tile > 0) blocks = (M + (int64_t)GPB * tile - 1) / ((int64_t)GPB * tile);
-    const int64_t cap = (int64_t)per_sm * m->num_sms;
-    if (blocks > cap) blocks = cap;
-    if (blocks < 1) blocks = 1;
-    if (tile > 0) cudaMemsetAsync(R.counter, 0, sizeof(unsigned long long), st);
-    kern<<<(unsigned)blocks, FAST_BLOCK, 0, st>>>(m->view, Q, cen, R.order, M, located, R.sum, tile,
-                                                 R.counter);
+    kern<<<(unsigned)blocks, FAST_BLOCK, smem, st>>>(m->view, Q, cen, R.order, M, R.nrows_dev, sink,
+                                                    LargeQueue{R.large}, R.sum, tile, R.counter);
 }
 
 // the structure-only (gradient) rows keep their own occupancy; the others
 // run at the mesh's tuned one
-template <class QT, class Sink, int PM, bool LOC>
+template <class QT, class Sink, int PM>
 void launch_fast_loc(const nif_dmesh *m, const QT *Q, int64_t M, const Centroid &cen,
                      const RowSet &R, const Sink &sink, cudaStream_t st) {
     if constexpr (!Sink::FULL)
-        launch_fast_occ<QT, Sink, PM, Sink::MIN_BLOCKS, LOC>(m, Q, M, cen, R, sink, st);
+        launch_fast_occ<QT, Sink, PM, Sink::MIN_BLOCKS>(m, Q, M, cen, R, sink, st);
     else if (m->tune.blocks_per_sm == OCC_LO)
-        launch_fast_occ<QT, Sink, PM, OCC_LO, LOC>(m, Q, M, cen, R, sink, st);
+        launch_fast_occ<QT, Sink, PM, OCC_LO>(m, Q, M, cen, R, sink, st);
     else
-        launch_fast_occ<QT, Sink, PM, OCC_HI, LOC>(m, Q, M, cen, R, sink, st);
+        launch_fast_occ<QT, Sink, PM, OCC_HI>(m, Q, M, cen, R, sink, st);
 }
 
-// With natinterp3d's signs and a located[] array in R (whose rows are a
-// plain order, not a queue), the rows are located by k_locate first and the
-// row kernel starts at the cavity; otherwise the row kernel locates.
+// the launch settings a row-kernel launch takes: the work-item tile (from
+// the mesh's or the batch's tuning) and the GPU's SM count
+struct Launch {
+    int tile;
+    int num_sms;
+};
+
+// one persistent launch of kernel `kern` over n rows (tiled schedule)
+template <class Kern, class... Args>
+void launch_rows(Kern kern, const Launch &lc, int64_t n, size_t smem, unsigned long long *counter,
+                 cudaStream_t st, Args... args) {
+    constexpr int GPB = FAST_BLOCK / FAST_G;
+    const int per_sm = resident_blocks(kern, FAST_BLOCK, smem);
+    const int tile = fit_tile(lc.tile, n, per_sm, lc.num_sms, GPB);
+    int64_t blocks = (n + GPB - 1) / GPB;
+    if (tile > 0) blocks = (n + (int64_t)GPB * tile - 1) / ((int64_t)GPB * tile);
+    const int64_t cap = (int64_t)per_sm * lc.num_sms;
+    if (blocks > cap) blocks = cap;
+    if (blocks < 1) blocks = 1;
+    if (tile > 0) cudaMemsetAsync(counter, 0, sizeof(unsigned long long), st);
+    kern<<<(unsigned)blocks, FAST_BLOCK, smem, st>>>(args..., tile, counter);
+}
+
+// resident blocks per SM of a row kernel with this sink: the mesh's setting,
+// except for the structure-only (gradient) rows, which keep their own
+template <class Sink, int OCC>
+constexpr int sink_occ() {
+    if constexpr (Sink::FULL)
+        return OCC;
+    else
+        return Sink::MIN_BLOCKS;
+}
+
+// The split row over positions [0, M) of R.order, whose rows `rows` maps to
+// their meshes: k_locate over all rows, then per chunk of REC_CHUNK rows the
+// cavity records and the volumes.  Rows whose cavity exceeds a record are
+// left in `wide` (count in R.sum->wide_count) for the fused kernel.
+template <class QT, class Rows, class Sink, int OCC>
+void launch_split(const Launch &lc, const Rows &rows, const QT *Q, int64_t M, const RowSet &R,
+                  RowHead *heads, RowEntry *ents, int *wide, const Sink &sink, cudaStream_t st) {
+    constexpr int GPB = FAST_BLOCK / FAST_G;
+    constexpr int COCC = NIF_CAV_OCC > 0 ? NIF_CAV_OCC : OCC;
+    constexpr int VOCC = sink_occ<Sink, (NIF_VOL_OCC > 0 ? NIF_VOL_OCC : OCC)>();
+    int *located = const_cast<int *>(R.located);
+    launch_rows(k_locate<QT, Rows>, lc, M, 0, R.counter, st, rows, Q, R.order, M, located, R.sum);
+    for (int64_t c0 = 0; c0 < M; c0 += REC_CHUNK) {
+        const int64_t n = min((int64_t)REC_CHUNK, M - c0);
+        launch_rows(k_rows_cavity<QT, Rows, COCC>, lc, n, GPB * sizeof(CavWS), R.counter, st, rows, Q,
+                    R.order + c0, n, (const int *)located, heads, ents, wide, LargeQueue{R.large},
+                    R.sum);
+        launch_rows(k_rows_volume<QT, Rows, Sink, VOCC>, lc, n, GPB * sizeof(VolWS), R.counter, st,
+                    rows, Q, R.order + c0, n, (const RowHead *)heads, (const RowEntry *)ents, sink,
+                    LargeQueue{R.large}, R.sum);
+    }
+}
+
+// With natinterp3d's signs, a located[] array and record buffers (and rows
+// that are a plain order, not a queue), the rows are located by k_locate and
+// then run through the split row kernels; otherwise the fused row kernel
+// takes them whole.
 template <class QT, class Sink, int PM>
 void launch_fast(const nif_dmesh *m, const QT *Q, int64_t M, const Centroid &cen,
-                 const RowSet &R, const Sink &sink, cudaStream_t st) {
+                 const RowSet &R, const Sink &sink, cudaStream_t st, RowHead *heads = nullptr,
+                 RowEntry *ents = nullptr, int *wide = nullptr) {
     if constexpr (PM == PM_PLAIN) {
-        if (R.located && !R.nrows_dev) {
-            launch_locate(m, Q, M, cen, R, const_cast<int *>(R.located), st);
-            launch_fast_loc<QT, Sink, PM, true>(m, Q, M, cen, R, sink, st);
+        if (R.located && heads && !R.nrows_dev) {
+            const Launch lc{m->tune.tile, m->num_sms};
+            const OneMesh rows{m->view, cen};
+            if (m->tune.blocks_per_sm == OCC_LO)
+                launch_split<QT, OneMesh, Sink, OCC_LO>(lc, rows, Q, M, R, heads, ents, wide, sink, st);
+            else
+                launch_split<QT, OneMesh, Sink, OCC_HI>(lc, rows, Q, M, R, heads, ents, wide, sink, st);
+            // rows whose cavity exceeds a record: the fused row kernel (which
+            // queues what exceeds its own capacities for the large kernel)
+            const RowSet W{wide, &R.sum->wide_count, R.large, R.sum, R.counter, nullptr};
+            launch_fast_loc<QT, Sink, PM_PLAIN>(m, Q, M, cen, W, sink, st);
             return;
         }
     }
-    launch_fast_loc<QT, Sink, PM, false>(m, Q, M, cen, R, sink, st);
+    launch_fast_loc<QT, Sink, PM>(m, Q, M, cen, R, sink, st);
 }
 
 // fast rows (filtered when the mesh's predicate mode is not the default),
@@ -1489,7 +1750,7 @@ template <class QT, class Sink>
 void run_rows(const nif_dmesh *m, const QT *Q, int64_t M, const Centroid &cen, const QueryLayout &L,
               const Sink &sink, cudaStream_t st, int large_groups = LARGE_GROUPS) {
     if (m->view.pmode == PRED_FAST)
-        launch_fast<QT, Sink, PM_PLAIN>(m, Q, M, cen, all_rows(L), sink, st);
+        launch_fast<QT, Sink, PM_PLAIN>(m, Q, M, cen, all_rows(L), sink, st, L.heads, L.ents, L.wide);
     else
         launch_fast<QT, Sink, PM_FILTER>(m, Q, M, cen, all_rows(L), sink, st);
     prof_mark(2, st);
@@ -2361,14 +2622,6 @@ NIF_EXPORT int nif_query_grad(const nif_dmesh *m, const void *d_queries, int que
 namespace nif {
 
 
-__device__ __forceinline__ int find_problem(const int64_t *__restrict__ off, int P, int64_t i) {
-    int lo = 0, hi = P;  // off[lo] <= i < off[hi]
-    while (hi - lo > 1) {
-        const int mid = (lo + hi) >> 1;
-        if (off[mid] <= i) lo = mid; else hi = mid;
-    }
-    return lo;
-}
 
 __device__ __forceinline__ int bucket_bits_dev(int64_t M) {
     int b = 1;
@@ -2442,9 +2695,11 @@ template <class QT, class Sink, int PM, int OCC>
 __global__ void __launch_bounds__(FAST_BLOCK, OCC)
     k_rows_batch(const MeshView *__restrict__ views, const int64_t *__restrict__ qoff, int P,
                  const QT *__restrict__ Q, const double *__restrict__ cens,
-                 const int *__restrict__ order, int64_t nrows, Sink sink, LargeQueue lq,
-                 DevSummary *sum, unsigned long long *counter, int tile) {
+                 const int *__restrict__ order, int64_t nrows, const int *nrows_dev, Sink sink,
+                 LargeQueue lq, DevSummary *sum, unsigned long long *counter, int tile) {
     extern __shared__ __align__(16) unsigned char smem[];
+    // a row count known only on the device (a queue's length) bounds nrows
+    if (nrows_dev) nrows = min(nrows, (int64_t)*nrows_dev);
     constexpr int G = FAST_G;
     constexpr int GPB = FAST_BLOCK / G;
     __shared__ MeshView sview[GPB];
@@ -2458,9 +2713,9 @@ __global__ void __launch_bounds__(FAST_BLOCK, OCC)
         unsigned long long t = 0;
         if (g.lane == 0) t = atomicAdd(counter, 1ull);
         t = __shfl_sync(g.mask, t, 0, G);
-        const int64_t s0 = (int64_t)t * tile;
+        int64_t s0, s1;
+        tile_range(t, tile, nrows, (int64_t)gridDim.x * GPB * tile, s0, s1);
         if (s0 >= nrows) break;
-        const int64_t s1 = min(nrows, s0 + (int64_t)tile);
         for (int64_t s = s0; s < s1; s++) {
             const int64_t i = order[s];
             const int p = find_problem(qoff, P, i);
@@ -2552,6 +2807,11 @@ struct BatchLayout {
     int64_t *bbase;
     LargeWS *large_ws;
     double *exact;
+    // split rows (the default predicate mode): located tets, one chunk's
+    // records, rows whose cavity exceeds a record
+    int *located, *wide;
+    RowHead *heads;
+    RowEntry *ents;
 };
 
 BatchLayout carve_batch(Carve &c, int P, int64_t M) {
@@ -2569,13 +2829,19 @@ BatchLayout carve_batch(Carve &c, int P, int64_t M) {
     L.btotal = c.take<int>(2);
     L.large_ws = c.take<LargeWS>(LARGE_GROUPS);
     L.exact = c.take<double>((size_t)LARGE_GROUPS * NIF_EXACT_SCRATCH);
+    const int64_t m1 = M > 0 ? M : 1;
+    const int64_t ch = m1 < REC_CHUNK ? m1 : REC_CHUNK;
+    L.located = c.take<int>(m1);
+    L.wide = c.take<int>(m1);
+    L.heads = c.take<RowHead>(ch);
+    L.ents = c.take<RowEntry>(ch * REC_CAV);
     return L;
 }
 
 template <class QT, class Sink, int PM, int OCC>
 void launch_batch_rows_occ(const nif_dbatch *b, const QT *Q, int64_t M, const int64_t *qoff,
                            const double *cens, const Sink &sink, const BatchLayout &L,
-                           cudaStream_t st) {
+                           cudaStream_t st, const int *order, const int *nrows_dev) {
     constexpr int GPB = FAST_BLOCK / FAST_G;
     const size_t smem = GPB * sizeof(FastWS);
     auto kern = k_rows_batch<QT, Sink, PM, OCC>;
@@ -2585,17 +2851,22 @@ void launch_batch_rows_occ(const nif_dbatch *b, const QT *Q, int64_t M, const in
     int64_t blocks = (int64_t)per_sm * b->num_sms;
     if (blocks > want) blocks = want;
     if (blocks < 1) blocks = 1;
-    kern<<<(unsigned)blocks, FAST_BLOCK, smem, st>>>(b->d_views, qoff, b->P, Q, cens, L.order, M, sink,
-                                                    LargeQueue{L.large_list}, L.sum, L.counter, tile);
+    cudaMemsetAsync(L.counter, 0, sizeof(unsigned long long), st);
+    kern<<<(unsigned)blocks, FAST_BLOCK, smem, st>>>(b->d_views, qoff, b->P, Q, cens, order, M, nrows_dev,
+                                                    sink, LargeQueue{L.large_list}, L.sum, L.counter,
+                                                    tile);
 }
 
+// the fused batch row kernel over positions [0, M) of `order` (bounded by
+// *nrows_dev where that is set)
 template <class QT, class Sink, int PM>
 void launch_batch_rows(const nif_dbatch *b, const QT *Q, int64_t M, const int64_t *qoff,
-                       const double *cens, const Sink &sink, const BatchLayout &L, cudaStream_t st) {
+                       const double *cens, const Sink &sink, const BatchLayout &L, cudaStream_t st,
+                       const int *order, const int *nrows_dev = nullptr) {
     if (b->tune.blocks_per_sm == OCC_LO)
-        launch_batch_rows_occ<QT, Sink, PM, OCC_LO>(b, Q, M, qoff, cens, sink, L, st);
+        launch_batch_rows_occ<QT, Sink, PM, OCC_LO>(b, Q, M, qoff, cens, sink, L, st, order, nrows_dev);
     else
-        launch_batch_rows_occ<QT, Sink, PM, OCC_HI>(b, Q, M, qoff, cens, sink, L, st);
+        launch_batch_rows_occ<QT, Sink, PM, OCC_HI>(b, Q, M, qoff, cens, sink, L, st, order, nrows_dev);
 }
 
 template <class QT, class VT, class CT>
@@ -2614,10 +2885,21 @@ void batch_typed(const nif_dbatch *b, const void *q, int64_t M, const int64_t *q
     launch_scan<int>(L.bcount, nbk, L.bsum, L.btotal, L.bcount, st);
     k_scatter<<<blocks_for(M, 256), 256, 0, st>>>(L.bucket, M, L.bcount, L.order);
     Sink sink{static_cast<const VT *>(v), koff, qoff, b->P, static_cast<CT *>(out), D};
-    if (b->filtered)
-        launch_batch_rows<QT, Sink, PM_FILTER>(b, Q, M, qoff, cens, sink, L, st);
-    else
-        launch_batch_rows<QT, Sink, PM_PLAIN>(b, Q, M, qoff, cens, sink, L, st);
+    if (b->filtered) {
+        launch_batch_rows<QT, Sink, PM_FILTER>(b, Q, M, qoff, cens, sink, L, st, L.order);
+    } else {
+        // the split row kernels, rows mapped to their problems' meshes; then
+        // the rows whose cavity exceeds a record through the fused kernel
+        const Launch lc{b->tune.tile, b->num_sms};
+        const ManyMeshes rows{b->d_views, qoff, b->P, cens};
+        const RowSet R{L.order, nullptr, L.large_list, L.sum, L.counter, L.located};
+        if (b->tune.blocks_per_sm == OCC_LO)
+            launch_split<QT, ManyMeshes, Sink, OCC_LO>(lc, rows, Q, M, R, L.heads, L.ents, L.wide, sink, st);
+        else
+            launch_split<QT, ManyMeshes, Sink, OCC_HI>(lc, rows, Q, M, R, L.heads, L.ents, L.wide, sink, st);
+        launch_batch_rows<QT, Sink, PM_PLAIN>(b, Q, M, qoff, cens, sink, L, st, L.wide,
+                                              &L.sum->wide_count);
+    }
     k_rows_batch_large<QT, Sink><<<LARGE_GROUPS, 32, 0, st>>>(b->d_views, qoff, b->P, Q, cens,
                                                              LargeQueue{L.large_list}, sink,
                                                              L.large_ws, L.exact, L.sum);

@@ -486,6 +486,72 @@ struct Workspace {
     int16_t vh_slot[VH_];
 };
 
+// Workspaces of the split row (k_rows_cavity, then k_rows_volume): the same
+// member names as Workspace, each holding only what its phase uses.
+template <int HS_, int CAV_, int G_, class SlotT, class CavT>
+struct CavWorkspace {
+    static constexpr int HS = HS_;
+    static constexpr int QCAP = HS_ * 3 / 4;
+    static constexpr int CAV = CAV_;
+    static constexpr int STACK = 4 * CAV_ + 1;
+    static constexpr int G = G_;
+    using slot_t = SlotT;
+    using cav_t = CavT;
+    union U {
+        struct {
+            int hkey[HS_];
+            CavT hval[HS_];
+            SlotT queue[HS_ * 3 / 4];
+        } a;
+        struct {
+            CavT stack[4 * CAV_ + 1];
+        } r;
+    } u;
+    int cav_tet[CAV_];
+    alignas(4) CavT cav_nbr[4 * CAV_];
+    CavT order[CAV_];
+    CavT pos[CAV_];
+};
+
+template <int CAV_, int BF_, int NBR_, int VH_, int G_>
+struct VolWorkspace {
+    static constexpr int CAV = CAV_;
+    static constexpr int BF = BF_;
+    static constexpr int NBR = NBR_;
+    static constexpr int VH = VH_;
+    static constexpr int G = G_;
+    union U {
+        double buf[4 * G_ * 10 / 8];  // the fold's item buffer (4 G terms + slots); sink staging
+    } u;
+    double acc[NBR_];
+    int cav_tet[CAV_];  // cavity tets in visiting order
+    int nbr_vid[NBR_];
+    int vh_key[VH_];
+    int vh_first[VH_];
+    uint16_t bface[BF_];
+    int16_t vh_slot[VH_];
+    uint8_t bmask[CAV_];  // boundary faces of each cavity tet, one bit per face
+};
+
+// One row between k_rows_cavity and k_rows_volume: a header and, per cavity
+// tet in natinterp3d's visiting order, the tet, the fcc[] indices of its
+// faces' circumcentres as natinterp3d's face cache returns them, and which
+// of its faces bound the cavity.
+constexpr int REC_CAV = 48;  // cavity tets a record holds (larger cavities take the large kernel)
+constexpr int RS_OK = 0, RS_OUTSIDE = 1, RS_WALK = 2, RS_QUEUED = 3;
+struct __align__(16) RowHead {
+    int ncav;   // cavity tets (0: the coincident-vertex row)
+    int start;  // located tet
+    int state;  // RS_*
+    int pad;
+};
+struct __align__(32) RowEntry {
+    int4 fp;
+    int tet;
+    unsigned bmask;
+    int pad[2];
+};
+
 __device__ __forceinline__ unsigned mix_hash(int key) {
     return (unsigned)key * 2654435761u;
 }
@@ -725,34 +791,20 @@ __device__ int locate(const MeshView &M, const dv3 q, const Grp<G> &g, int *scra
     }
 }
 
-// The Sibson row of centred query q.  On ST_OK the row is ws.nbr_vid[0..nnb)
-// with normalised weights ws.acc[0..nnb), in natinterp3d's column order.
-// With FULL = false only the combinatorial part is built (cavity, visiting
-// order, boundary faces, neighbours in column order) and no volume is
-// computed; the query-gradient kernel needs nothing more.  PM selects the
-// predicate variant (PM_*); PM_RESOLVE needs xs, NIF_EXACT_SCRATCH doubles of
-// global scratch owned by this group.  With LOC the query was located by
-// k_locate (PM_PLAIN only): `located` is its tet, and this code holds no
-// point location of its own.
-template <int G, class W, bool FULL = true, int PM = PM_PLAIN, bool LOC = false>
-__device__ RowInfo sibson_row(const MeshView &M, const dv3 q, W &ws, const Grp<G> &g,
-                              double *xs = nullptr, int located = 0) {
-    static_assert(!LOC || PM == PM_PLAIN, "located rows use natinterp3d's signs");
+// Steps 2 of the row: the cavity of q around tet `start` (natinterp3d's
+// findCavity, natural_insertionfree.c:486-551) by a parallel flood over the
+// tested-tet hash, then natinterp3d's LIFO visiting order replayed on it.
+// Returns the number of cavity tets, ws.cav_tet[c] their tets, ws.order[o]
+// the cavity index of the o-th visited, ws.pos its inverse and ws.cav_nbr
+// [4c + f] the cavity index of neighbour f of cavity tet c (-1 outside).  On
+// overflow / an uncertain test (PM_FILTER) r.status is set; an empty cavity
+// (0) leaves the order unset.
+template <int G, class W, int PM>
+__device__ int flood_replay(const MeshView &M, const dv3 q, W &ws, const Grp<G> &g, const int start,
+                            RowInfo &r, const bool on_face, double *xs) {
     using cav_t = typename W::cav_t;
     using slot_t = typename W::slot_t;
-    RowInfo r{ST_OK, 0, 0, false, false, 0.0, 0, 0, 0, 0, 0};
-    // filters run only for the non-default modes
     const bool filt = PM != PM_PLAIN && M.pmode != PRED_FAST;
-    bool on_face = false;  // PRED_EXACT: a face test of the located tet is exactly zero
-
-    // ---- 1. point location -------------------------------------------------
-    int t = located;
-    if constexpr (!LOC) {
-        t = locate<G, PM>(M, q, g, reinterpret_cast<int *>(ws.acc), r, on_face, xs);
-        if (r.status != ST_OK || r.outside) return r;
-    }
-    const int start = t;
-
     // ---- 2. cavity: parallel flood over the tested-tet hash ----------------
     // While a cavity tet's four neighbours are inserted into the hash, the
     // slot of each is kept in nsl[4c+f] (aliasing cav_nbr, which is filled
@@ -805,7 +857,7 @@ __device__ RowInfo sibson_row(const MeshView &M, const dv3 q, W &ws, const Grp<G
         if constexpr (PM == PM_FILTER) {
             if (g.any(unc)) {
                 r.status = ST_UNCERTAIN;
-                return r;
+                return 0;
             }
         } else if constexpr (PM == PM_RESOLVE) {
             if (filt && g.any(unc)) {
@@ -856,30 +908,9 @@ __device__ RowInfo sibson_row(const MeshView &M, const dv3 q, W &ws, const Grp<G
     g.sync();
     if (overflow) {
         r.status = ST_CAPACITY;
-        return r;
+        return 0;
     }
-
-    if (ncav == 0) {
-        // coincident-vertex path (natural_insertionfree.c:596-622): an empty
-        // cavity means the query may sit exactly on a vertex of the start tet
-        bool co = false;
-        int v = -1;
-        if (g.lane < 4) {
-            v = comp(M.tv[start], g.lane);
-            co = v < M.n && veq(vload(M, v), q);
-        }
-        const unsigned cm = g.ballot(co);
-        const int nco = __popc(cm);
-        if (co) {
-            const int s = __popc(cm & g.lt());
-            ws.nbr_vid[s] = v;
-            ws.acc[s] = fdiv(1.0, (double)nco);
-        }
-        g.sync();
-        r.nnb = nco;
-        r.coincident = true;
-        return r;
-    }
+    if (ncav == 0) return 0;
 
     // cavity-local neighbour table: cav_nbr[4c+f] = cavity index of s[f] or -1
     // (every neighbour slot recorded by the flood has been tested by now)
@@ -943,16 +974,74 @@ __device__ RowInfo sibson_row(const MeshView &M, const dv3 q, W &ws, const Grp<G
     }
     g.sync();
 
+    return ncav;
+}
+
+// The coincident-vertex row (natural_insertionfree.c:596-622): an empty
+// cavity means the query may sit exactly on a vertex of the start tet; the
+// row is 1/n on each of the n data vertices of that tet equal to q.
+template <int G, class W>
+__device__ void coincident_row(const MeshView &M, const dv3 q, W &ws, const Grp<G> &g, int start,
+                               RowInfo &r) {
+    bool co = false;
+    int v = -1;
+    if (g.lane < 4) {
+        v = comp(M.tv[start], g.lane);
+        co = v < M.n && veq(vload(M, v), q);
+    }
+    const unsigned cm = g.ballot(co);
+    const int nco = __popc(cm);
+    if (co) {
+        const int s = __popc(cm & g.lt());
+        ws.nbr_vid[s] = v;
+        ws.acc[s] = fdiv(1.0, (double)nco);
+    }
+    g.sync();
+    r.nnb = nco;
+    r.coincident = true;
+}
+
+// The circumcentres of the 4 faces of cavity tet c as natinterp3d's face
+// cache returns them (natural_insertionfree.c:233-253), as fcc[] indices
+// (4 T < 2^31: nif_dmesh_create limits T): for a face shared with another
+// cavity tet, the copy cached by whichever of the two natinterp3d visits first
+// (its mirror slot is in tinfo), else the tet's own.  Needs ws.pos.
+template <class W>
+__device__ __forceinline__ void face_cc_choice(const MeshView &M, const W &ws, int c, int (&fp)[4]) {
+    const int tt = ws.cav_tet[c];
+    const uint32_t info = M.tinfo[tt];
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        const int j = 3 - i;
+        const int nc = ws.cav_nbr[4 * c + j];
+        if (nc >= 0 && ws.pos[nc] < ws.pos[c]) {
+            const int jm = (info >> (8 + 2 * j)) & 3;
+            fp[i] = 4 * ws.cav_tet[nc] + (3 - jm);
+        } else {
+            fp[i] = 4 * tt + i;
+        }
+    }
+}
+
+// Steps 3-5 of the row: boundary faces in visiting order, the natural
+// neighbours in first-seen order, and (FULL) the stolen volumes folded in
+// natinterp3d's order and normalised.  The caller describes the cavity:
+//   face(k, c)       whether face k & 3 of the (k >> 2)-th tet in visiting
+//                    order is a boundary face; c = that tet's index into
+//                    ws.cav_tet
+//   tet_fp(o, c, fp) the o-th tet in visiting order (index c into
+//                    ws.cav_tet) and the fcc[] indices of its four faces as
+//                    natinterp3d's face cache returns them
+template <int G, class W, bool FULL, class FaceFn, class FpFn>
+__device__ RowInfo row_volumes(const MeshView &M, const dv3 q, W &ws, const Grp<G> &g, const int ncav,
+                               RowInfo r, FaceFn face, FpFn tet_fp) {
     // ---- 3. boundary faces (cavity order, then face order) ------------------
     int nbf = 0;
     for (int k0 = 0; k0 < 4 * ncav; k0 += G) {
         const int k = k0 + g.lane;
         bool isb = false;
         int c = 0;
-        if (k < 4 * ncav) {
-            c = ws.order[k >> 2];
-            isb = ws.cav_nbr[4 * c + (k & 3)] < 0;
-        }
+        if (k < 4 * ncav) isb = face(k, c);
         const unsigned bm = g.ballot(isb);
         const int b = nbf + __popc(bm & g.lt());
         if (isb && b < W::BF) ws.bface[b] = (uint16_t)((c << 2) | (k & 3));
@@ -1063,27 +1152,10 @@ __device__ RowInfo sibson_row(const MeshView &M, const dv3 q, W &ws, const Grp<G
             const int o = o0 + g.lane;
             const int nt_round = min(G, ncav - o0);
             if (o < ncav) {
-                const int c = ws.order[o];
+                int c, fp[4];
+                tet_fp(o, c, fp);
                 const int tt = ws.cav_tet[c];
                 const int4 p = M.tv[tt];
-                const uint32_t info = M.tinfo[tt];
-                // circumcentres of the 4 faces as natinterp3d's face cache returns
-                // them (natural_insertionfree.c:233-253): for a face shared with
-                // another cavity tet, the copy cached by whichever of the two
-                // natinterp3d visits first (its mirror slot is in tinfo); as
-                // fcc[] indices (4 T < 2^31: nif_dmesh_create limits T)
-                int fp[4];
-#pragma unroll
-                for (int i = 0; i < 4; i++) {
-                    const int j = 3 - i;
-                    const int nc = ws.cav_nbr[4 * c + j];
-                    if (nc >= 0 && ws.pos[nc] < ws.pos[c]) {
-                        const int jm = (info >> (8 + 2 * j)) & 3;
-                        fp[i] = 4 * ws.cav_tet[nc] + (3 - jm);
-                    } else {
-                        fp[i] = 4 * tt + i;
-                    }
-                }
 #pragma unroll 1
                 for (int vi = 0; vi < 4; vi++) {
                     const int v = comp(p, vi);
@@ -1165,6 +1237,105 @@ __device__ RowInfo sibson_row(const MeshView &M, const dv3 q, W &ws, const Grp<G
     r.nnb = nnb;
     r.total = total;
     return r;
+}
+
+// The Sibson row of centred query q.  On ST_OK the row is ws.nbr_vid[0..nnb)
+// with normalised weights ws.acc[0..nnb), in natinterp3d's column order.
+// With FULL = false only the combinatorial part is built (cavity, visiting
+// order, boundary faces, neighbours in column order) and no volume is
+// computed; the query-gradient kernel needs nothing more.  PM selects the
+// predicate variant (PM_*); PM_RESOLVE needs xs, NIF_EXACT_SCRATCH doubles of
+// global scratch owned by this group.  (The split kernels, k_rows_cavity and
+// k_rows_volume, run the same steps on located rows.)
+template <int G, class W, bool FULL = true, int PM = PM_PLAIN>
+__device__ RowInfo sibson_row(const MeshView &M, const dv3 q, W &ws, const Grp<G> &g,
+                              double *xs = nullptr) {
+    RowInfo r{ST_OK, 0, 0, false, false, 0.0, 0, 0, 0, 0, 0};
+    bool on_face = false;  // PRED_EXACT: a face test of the located tet is exactly zero
+
+    // ---- 1. point location -------------------------------------------------
+    const int start = locate<G, PM>(M, q, g, reinterpret_cast<int *>(ws.acc), r, on_face, xs);
+    if (r.status != ST_OK || r.outside) return r;
+
+    // ---- 2. cavity and natinterp3d's visiting order ---------------------------
+    const int ncav = flood_replay<G, W, PM>(M, q, ws, g, start, r, on_face, xs);
+    if (r.status != ST_OK) return r;
+    if (ncav == 0) {
+        coincident_row<G>(M, q, ws, g, start, r);
+        return r;
+    }
+    auto face = [&](int k, int &c) {
+        c = ws.order[k >> 2];
+        return ws.cav_nbr[4 * c + (k & 3)] < 0;
+    };
+    auto tet_fp = [&](int o, int &c, int (&fp)[4]) {
+        c = ws.order[o];
+        face_cc_choice(M, ws, c, fp);
+    };
+    return row_volumes<G, W, FULL>(M, q, ws, g, ncav, r, face, tet_fp);
+}
+
+// The split row, part 1: cavity and visiting order of q around its located
+// tet, written as a record (head, entries[REC_CAV]).  Returns REC_DONE, or
+// REC_WIDE where the cavity fits the shared-memory capacities but not the
+// record (the caller queues the row for the fused row kernel), or REC_LARGE
+// where it exceeds the shared-memory capacities (the large kernel's).
+constexpr int REC_DONE = 0, REC_WIDE = 1, REC_LARGE = 2;
+template <int G, class W>
+__device__ int cavity_record(const MeshView &M, const dv3 q, W &ws, const Grp<G> &g, int start,
+                             RowHead &head, RowEntry *__restrict__ ent) {
+    RowInfo r{ST_OK, 0, 0, false, false, 0.0, 0, 0, 0, 0, 0};
+    const int ncav = flood_replay<G, W, PM_PLAIN>(M, q, ws, g, start, r, false, nullptr);
+    if (r.status != ST_OK) return REC_LARGE;
+    if (ncav > REC_CAV) return REC_WIDE;
+    head.ncav = ncav;
+    for (int o = g.lane; o < ncav; o += G) {
+        const int c = ws.order[o];
+        int fp[4];
+        face_cc_choice(M, ws, c, fp);
+        unsigned bm = 0;
+#pragma unroll
+        for (int f = 0; f < 4; f++) bm |= (ws.cav_nbr[4 * c + f] < 0 ? 1u : 0u) << f;
+        RowEntry e;
+        e.fp = make_int4(fp[0], fp[1], fp[2], fp[3]);
+        e.tet = ws.cav_tet[c];
+        e.bmask = bm;
+        e.pad[0] = e.pad[1] = 0;
+        ent[o] = e;
+    }
+    g.sync();
+    return REC_DONE;
+}
+
+// The split row, part 2: from a record of part 1 (state RS_OK) the row as
+// sibson_row returns it (steps 3-5, or the coincident-vertex row).
+template <int G, class W, bool FULL>
+__device__ RowInfo volume_row(const MeshView &M, const dv3 q, W &ws, const Grp<G> &g,
+                              const RowHead &head, const RowEntry *__restrict__ ent) {
+    RowInfo r{ST_OK, 0, 0, false, false, 0.0, 0, 0, 0, 0, 0};
+    const int ncav = head.ncav;
+    if (ncav == 0) {
+        coincident_row<G>(M, q, ws, g, head.start, r);
+        return r;
+    }
+    for (int o = g.lane; o < ncav; o += G) {
+        ws.cav_tet[o] = ent[o].tet;
+        ws.bmask[o] = (uint8_t)ent[o].bmask;
+    }
+    g.sync();
+    auto face = [&](int k, int &c) {
+        c = k >> 2;
+        return ((ws.bmask[c] >> (k & 3)) & 1u) != 0u;
+    };
+    auto tet_fp = [&](int o, int &c, int (&fp)[4]) {
+        c = o;
+        const int4 f = ent[o].fp;
+        fp[0] = f.x;
+        fp[1] = f.y;
+        fp[2] = f.z;
+        fp[3] = f.w;
+    };
+    return row_volumes<G, W, FULL>(M, q, ws, g, ncav, r, face, tet_fp);
 }
 
 }  // namespace nif
