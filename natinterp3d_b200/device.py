@@ -164,11 +164,13 @@ class DeviceMesh:
             out = out + (summ.as_dict(),)
         return out
 
-    def interpolate(self, q, values, centroid, return_summary=False, check=True, sync=True):
+    def interpolate(self, q, values, centroid, return_summary=False, check=True, sync=True, ws=None):
         """out[M, D] = W(q) @ values without materialising W (device tensors).
 
         With ``sync=False`` and ``return_summary`` the row counters are left on
-        the device (returned as a pending handle for :meth:`raise_pending`)."""
+        the device (returned as a pending handle for :meth:`raise_pending`).
+        ``ws``: a workspace of at least ``workspace_bytes(M, NIF_MODE_INTERP)``
+        bytes to use instead of a new one."""
         _check_device_tensor(q, self.device, 'queries')
         _check_device_tensor(values, self.device, 'values')
         q = q.contiguous()
@@ -185,7 +187,8 @@ class DeviceMesh:
         M, D = int(q.shape[0]), int(v.shape[1])
         cen = (ctypes.c_double * 3)(*[float(c) for c in centroid])
         with torch.cuda.device(self.device):
-            ws = self._workspace(M, N.NIF_MODE_INTERP)
+            if ws is None:
+                ws = self._workspace(M, N.NIF_MODE_INTERP)
             out = torch.empty((M, D), dtype=out_dtype, device=self.device)
             summ = N.Summary()
             want = check or (return_summary and sync)

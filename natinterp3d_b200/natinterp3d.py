@@ -30,11 +30,53 @@ import numpy as np
 import scipy.sparse
 import torch
 
+from . import _native as N
 from ._native import HostMesh
 from .device import DeviceMesh
 
 _FLOATS = (np.dtype(np.float32), np.dtype(np.float64))
 PIPELINE_CHUNK = 1 << 21  # queries per chunk of the pipelined host interpolation
+
+
+HOST_STAGE = 1 << 24  # bytes per pinned staging buffer of device-to-host copies
+
+
+def _to_host(t):
+    """A device tensor as a numpy array in pageable host memory: copied
+    through two reused pinned staging buffers on a side stream, the copy of
+    one piece overlapping the host-side copy (multithreaded) of the previous;
+    large results come back several times faster than a direct pageable copy,
+    whose first touch of fresh host pages is single-threaded."""
+    t = t.contiguous()
+    n = t.numel()
+    out = torch.empty(t.shape, dtype=t.dtype)
+    if n * t.element_size() <= HOST_STAGE:
+        out.copy_(t)
+        return out.numpy()
+    flat, dst = t.view(-1), out.view(-1)
+    step = HOST_STAGE // t.element_size()
+    dev = t.device
+    copy = torch.cuda.Stream(device=dev)
+    copy.wait_stream(torch.cuda.current_stream(dev))
+    stage = [torch.empty(step, dtype=t.dtype, pin_memory=True) for _ in range(2)]
+    done = [None, None]
+    pieces = [(a, min(n, a + step)) for a in range(0, n, step)]
+
+    def issue(k):
+        a, b = pieces[k]
+        with torch.cuda.stream(copy):
+            stage[k % 2][:b - a].copy_(flat[a:b], non_blocking=True)
+            done[k % 2] = torch.cuda.Event()
+            done[k % 2].record(copy)
+
+    issue(0)
+    for k, (a, b) in enumerate(pieces):
+        if k + 1 < len(pieces):
+            issue(k + 1)
+        done[k % 2].synchronize()
+        dst[a:b].copy_(stage[k % 2][:b - a])
+    flat.record_stream(copy)
+    return out.numpy()
 
 
 def pipeline_bounds(M, chunk):
@@ -265,8 +307,7 @@ class Interpolator:
         rowptr, cols, vals = dm.weights_csr(qd, self._centroid, vals_dtype=torch.float64)
         M = q.shape[0]
         W = scipy.sparse.csr_matrix(
-            (vals.cpu().numpy(), cols.cpu().numpy(), rowptr.cpu().numpy()),
-            shape=(M, self.n_keys))
+            (_to_host(vals), _to_host(cols), _to_host(rowptr)), shape=(M, self.n_keys))
         # natinterp3d.py:117; a dtype-changing astype also canonicalises the
         # CSR (sorted columns), exactly as it does for natinterp3d's result
         return W.astype(out_dtype, copy=False)
@@ -309,6 +350,9 @@ class Interpolator:
         compute = torch.cuda.current_stream(dev)
         copy = torch.cuda.Stream(device=dev)
         staging = [torch.empty((PIPELINE_CHUNK, D), dtype=odt, pin_memory=True) for _ in range(2)]
+        # two workspaces in turn: a chunk's counters are read (on the copy
+        # stream) before the chunk two later reuses its workspace
+        wss = [dm._workspace(PIPELINE_CHUNK, N.NIF_MODE_INTERP) for _ in range(2)]
         counters = []
         pending = None  # (slot, rows, device result, event, row-counter handle)
 
@@ -318,7 +362,6 @@ class Interpolator:
             with torch.cuda.stream(copy):
                 staging[slot][:b - a].copy_(res.reshape(b - a, D), non_blocking=True)
                 res.record_stream(copy)
-                handle[1].record_stream(copy)
             copy.synchronize()
             out[a:b] = staging[slot][:b - a].numpy()
             # the chunk's row counters, read on the copy stream (the compute
@@ -334,7 +377,7 @@ class Interpolator:
                 compute.wait_event(loaded)
                 qd.record_stream(compute)
                 res, handle = dm.interpolate(qd, vd, self._centroid, return_summary=True,
-                                             check=False, sync=False)
+                                             check=False, sync=False, ws=wss[k % 2])
                 done = torch.cuda.Event()
                 done.record(compute)
                 if pending is not None:
