@@ -37,10 +37,12 @@ METRIC = 'Sibson queries/s at 1M keys (plain, fwd+bwd, batched) vs CPU OpenMP, 1
 WORKLOAD = ('plain interpolate at scale: {keys:,} keys U[0,1]^3 float64, {queries:,} queries '
             'U[0.02,0.98]^3 float64, values D={dim} float32 N(0,1), seed {seed}')
 
-# DRAM bytes (read + write) per query of one k_rows_fast launch, from an ncu
-# capture of the plain workload (profiles/launches_1M_keys_10M_queries.md)
-TRAFFIC_PER_QUERY = 4.4257e9 / 10_000_000
-TRAFFIC_SOURCE = '1M keys / 10M queries, profiles/launches_1M_keys_10M_queries.md'
+# DRAM bytes (read + write) per row of one launch, from the ncu captures in
+# profiles/ (TRAFFIC_SOURCE)
+TRAFFIC_PER_ROW = {'k_rows_volume': (1.14e9 + 68.19e6) / 1_000_000}
+TRAFFIC_SOURCE = ('one 1,000,000-row k_rows_volume launch of the 1M-key / 10M-query workload '
+                  '(dram__bytes_read.sum + dram__bytes_write.sum, 1 pass; '
+                  'profiles/k_rows_volume_200k_keys_2M_queries.md)')
 
 # FP64 operations per unit of work, counted as natinterp3d's C evaluates them
 # (each add, subtract, multiply and divide is one flop; no fused multiply-add)
@@ -161,22 +163,26 @@ class ClockSampler:
 
 # ---------------------------------------------------------------------------
 def flops_per_query(stats, gpu_walk_steps, n):
-    """Algorithmic FP64 flops per query of the GPU row kernel.
+    """Algorithmic FP64 flops per query of the row path, by kernel.
 
-    The kernel reads tet and face circumcentres from the per-mesh cache, so
-    per query it evaluates: 4 orientation tests per walk step, the insphere
-    tests, one virtual-tet circumcentre per boundary face, two fresh triangle
-    circumcentres and one subcell volume per new term, one subcell volume per
-    old term, one addition per term, and the normalisation."""
+    The kernels read tet and face circumcentres from the per-mesh cache, so
+    per query they evaluate: 4 orientation tests per walk step (k_locate),
+    the insphere tests (k_rows_cavity), and in k_rows_volume one virtual-tet
+    circumcentre per boundary face, two fresh triangle circumcentres and one
+    subcell volume per new term, one subcell volume per old term, one
+    addition per term, and the normalisation.  Returns {'locate', 'cavity',
+    'volume', 'total'} per query."""
     q = stats['queries']
     terms = stats['old_terms'] + stats['new_terms']
-    total = (4 * FLOPS['orient'] * gpu_walk_steps / n * q
-             + FLOPS['insphere'] * stats['insphere']
-             + FLOPS['tet_cc'] * stats['boundary']
-             + 2 * FLOPS['tri_cc'] * stats['new_terms']
-             + FLOPS['subcell'] * terms
-             + terms + 3 * stats['neighbours'] + 4 * q)
-    return total / q
+    locate = 4 * FLOPS['orient'] * gpu_walk_steps / n * q
+    cavity = FLOPS['insphere'] * stats['insphere']
+    volume = (FLOPS['tet_cc'] * stats['boundary']
+              + 2 * FLOPS['tri_cc'] * stats['new_terms']
+              + FLOPS['subcell'] * terms
+              + terms + 3 * stats['neighbours'] + 4 * q)
+    out = {'locate': locate / q, 'cavity': cavity / q, 'volume': volume / q}
+    out['total'] = sum(out.values())
+    return out
 
 
 def plain_config(args, world):
@@ -387,6 +393,63 @@ def leg_get_weights_small(local_rank, steps, warmup, cpu=True):
     return _weights_leg(interp, queries, steps, warmup, cpu, 100_000,
                         'get_weights: 10,000 keys U[0,1]^3, 100,000 queries U[0.05,0.95]^3, '
                         'float64, seed 0')
+
+
+def tet_set_digest(tet_v):
+    """(count, two order-independent 64-bit sums) of a tet set: the sorted
+    vertex quadruple of each tet mixed by two odd-multiplier hashes."""
+    t = np.sort(np.asarray(tet_v), axis=1).astype(np.uint64)
+    c1 = np.array([0x9E3779B97F4A7C15, 0xC2B2AE3D27D4EB4F, 0x165667B19E3779F9,
+                   0xD6E8FEB86659FD93], dtype=np.uint64)
+    c2 = np.array([0xFF51AFD7ED558CCD, 0xC4CEB9FE1A85EC53, 0x94D049BB133111EB,
+                   0xBF58476D1CE4E5B9], dtype=np.uint64)
+    with np.errstate(over='ignore'):
+        h1 = (t * c1).sum(axis=1, dtype=np.uint64)
+        h2 = (t * c2).sum(axis=1, dtype=np.uint64)
+        h1 ^= h1 >> np.uint64(29)
+        h2 ^= h2 >> np.uint64(31)
+        h1 *= np.uint64(0xBF58476D1CE4E5B9)
+        h2 *= np.uint64(0x94D049BB133111EB)
+        return int(t.shape[0]), int(h1.sum(dtype=np.uint64)), int(h2.sum(dtype=np.uint64))
+
+
+def leg_gpu_construction(keys, interp, host_build_s, local_rank):
+    """natinterp3d's tetrahedralization of the bench keys built on the GPU
+    (``constructor='gpu'``) against natinterp3d's host constructor, which
+    built ``interp``'s mesh in ``host_build_s`` seconds: time, rounds, the
+    builder's exact checks, and whether the tet set equals natinterp3d's."""
+    import torch
+    from natinterp3d_b200.device import gpu_delaunay, GPUConstructionError
+    dev = torch.device('cuda', local_rank)
+    centered = keys - interp.centroid
+    gpu_delaunay(centered[:10_000], dev)  # first-use costs (module load) off the clock
+    torch.cuda.synchronize()
+    times = []
+    for _ in range(2):
+        t0 = time.perf_counter()
+        try:
+            (vxyz, tv, tn), info = gpu_delaunay(centered, dev)
+        except GPUConstructionError as e:
+            return {'unavailable': str(e)}
+        torch.cuda.synchronize()
+        times.append(time.perf_counter() - t0)
+        last = tv
+    t = min(times)
+    host_tv = interp.mesh_arrays[1]
+    same = (tet_set_digest(last.cpu().numpy()) == tet_set_digest(host_tv)
+            and np.array_equal(vxyz.cpu().numpy().view(np.uint8),
+                               interp.mesh_arrays[0].view(np.uint8)))
+    return {'value': keys.shape[0] / t, 'unit': 'keys/s', 'gpu_s': t,
+            'host_constructor_s': host_build_s, 'speedup_vs_host': host_build_s / t,
+            'tets': int(info['n_tets']), 'rounds': int(info['rounds']),
+            'max_cavity': int(info['max_cavity']),
+            'exact_evaluations': int(info['exact_evaluations']),
+            'checks': {k: int(info[k]) for k in ('bad_orientation', 'bad_adjacency',
+                                                  'non_delaunay_faces', 'cospherical_faces')},
+            'same_tets_and_vertices_as_natinterp3d': bool(same),
+            'config': {'workload': 'Delaunay tetrahedralization of the plain workload\'s keys '
+                                   '(+ natinterp3d\'s super-simplex), wall clock with the result '
+                                   'on the device'}}
 
 
 def leg_fwdbwd(args, rank, local_rank, steps, warmup, cpu=True):
@@ -663,6 +726,8 @@ def main():
     # read once here: the loop itself never waits on the host)
     ph = (ctypes.c_double * 4)()
     have_phases = lib.nif_profile_read(ph) == 0
+    kms, kn = (ctypes.c_double * 4)(), (ctypes.c_double * 4)()
+    lib.nif_profile_kernels(kms, kn)
     lib.nif_profile_enable(0)
     ms = e0.elapsed_time(e1) / args.steps
     if dist is not None:
@@ -693,7 +758,21 @@ def main():
         fpq = flops_per_query(stats, summ['walk_steps'], M)
         fused, separate = ctypes.c_double(), ctypes.c_double()
         lib.nif_measure_fp64_peak(ctypes.byref(fused), ctypes.byref(separate))
-        achieved = fpq * M / (rows_ms * 1e-3) / 1e12 if rows_ms > 0 else None
+        # the dominant kernel, k_rows_volume: its launches take every row but
+        # the few the fused kernel takes (cavities wider than a record)
+        vol_rows = M - int(summ['rows_wide'])
+        vol_ms, vol_launches = kms[2], kn[2]
+        achieved = (fpq['volume'] * vol_rows / (vol_ms * 1e-3) / 1e12) if vol_ms > 0 else None
+        path_achieved = fpq['total'] * M / (rows_ms * 1e-3) / 1e12 if rows_ms > 0 else None
+        names = ['k_locate', 'k_rows_cavity', 'k_rows_volume', 'k_rows_fast']
+        kernels = {n: {'ms_per_step': kms[i], 'launches_per_step': kn[i],
+                       'share_of_rows_phase': kms[i] / rows_ms if rows_ms > 0 else None}
+                   for i, n in enumerate(names)}
+        for i, part in enumerate(['locate', 'cavity', 'volume']):
+            kernels[names[i]]['flops_per_query'] = fpq[part]
+        # bucketing (k_bucket, three scan kernels, k_scatter), the row kernels
+        # the profiler bracketed, and the large-row kernel
+        launches_per_step = int(round(5 + sum(kn) + 1))
         cpu = None if args.no_cpu_baseline else cpu_baseline(interp, queries, values)
         line = {
             'metric': METRIC, 'value': value, 'unit': 'queries/s', 'n_gpus': world,
@@ -710,26 +789,37 @@ def main():
                 'tune_s': round(tune_s, 2), 'tune_sample_ms': tune_times,
             },
             'roofline': {
-                'bound': 'fp64', 'kernel': 'k_rows_fast',
+                'bound': 'fp64', 'kernel': 'k_rows_volume',
                 'achieved': achieved, 'peak': separate.value, 'unit': 'TFLOP/s',
                 'frac': (achieved / separate.value) if achieved and separate.value else None,
                 'peak_fused_fma': fused.value,
                 'peak_note': 'measured on this GPU by nif_measure_fp64_peak: separately rounded '
                              'DMUL+DADD (the kernels never fuse, for bit parity)',
-                'flops_per_query': fpq, 'kernel_ms': rows_ms,
-                'phase_ms': {'bucketing': phases[0], 'rows_fast': rows_ms,
+                'flops_per_query': fpq['volume'],
+                'rows_per_launch': vol_rows / vol_launches if vol_launches else None,
+                'launch_ms': vol_ms / vol_launches if vol_launches else None,
+                # dram__bytes_read.sum + dram__bytes_write.sum of one
+                # k_rows_volume launch from an ncu capture (profiles/), per row,
+                # times this workload's rows per launch
+                'traffic': (TRAFFIC_PER_ROW['k_rows_volume'] * vol_rows / vol_launches
+                            if vol_launches else None),
+                'traffic_note': 'per launch; ncu capture of %s' % TRAFFIC_SOURCE,
+                'row_path': {
+                    'kernels': 'k_locate + k_rows_cavity + k_rows_volume (+ k_rows_fast)',
+                    'achieved': path_achieved, 'flops_per_query': fpq['total'],
+                    'frac': (path_achieved / separate.value) if path_achieved and separate.value
+                    else None,
+                    'ms_per_step': rows_ms,
+                },
+                'kernels': kernels,
+                'phase_ms': {'bucketing': phases[0], 'rows': rows_ms,
                              'rows_large': phases[2], 'epilogue': phases[3]},
-                # dram__bytes_read.sum + dram__bytes_write.sum of one k_rows_fast
-                # launch from an ncu capture of this workload (profiles/), scaled
-                # by this launch's query count
-                'traffic': TRAFFIC_PER_QUERY * M,
-                'traffic_note': 'ncu capture of one k_rows_fast launch, %s' % TRAFFIC_SOURCE,
             },
             'cpu_baseline': cpu,
             'e2e': {'value': M * world / e2e_sec, 'unit': 'queries/s',
                     'h2d_bytes_per_step': int(queries.nbytes + values.nbytes),
                     'd2h_bytes_per_step': int(out.nbytes)},
-            'gpu_launches': 7 * args.steps,
+            'gpu_launches': launches_per_step * args.steps,
             'clocks': clocks.summary(),
             'summary': {k: int(v) for k, v in summ.items() if k != 'nnz'},
         }
@@ -746,6 +836,8 @@ def main():
             del out
             legs['fwd+bwd'] = leg_fwdbwd(args, rank, local_rank, max(args.steps, 5),
                                          max(args.warmup, 3), cpu_on)
+            legs['gpu_construction_1M_keys'] = leg_gpu_construction(keys, interp, build_s,
+                                                                    local_rank)
             legs['batched'] = leg_batched(args, rank, local_rank, max(args.steps, 3),
                                           max(args.warmup, 3), cpu_on)
             line['legs'] = legs

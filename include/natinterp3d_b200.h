@@ -87,6 +87,42 @@ void *nif_mesh_native(const nif_mesh *h);
 /* libnif_cuda.so: device-resident mesh and query kernels                   */
 /* ======================================================================== */
 
+/* ---- GPU construction (opt-in; natinterp3d has no counterpart) ----------
+ * The Delaunay tetrahedralization of n centred keys plus natinterp3d's
+ * super-simplex (initSuperSimplex, delaunay.c:832-863), built on the device
+ * by parallel Bowyer-Watson insertion rounds with exact predicates, in the
+ * packed layout of nif_mesh_export (vxyz [n+4][3] with the super-simplex
+ * vertices at rows n..n+3; tet_v, tet_n [T][4] with natinterp3d's face
+ * order, delaunay.c:444-467).  For keys in general position this is the
+ * same set of tets natinterp3d's constructor (buildMesh, delaunay.c:108-161)
+ * produces; tet order and each tet's vertex rotation differ.  The result is
+ * checked on the device with exact predicates (positive orientation,
+ * neighbour symmetry, empty circumsphere across every interior face) and
+ * the counts reported in *info.  Returns NIF_ERR_DEGENERATE where an exact
+ * zero would decide the result (cospherical or coplanar keys that a cavity
+ * meets, duplicate keys, zero extent): natinterp3d then perturbs keys
+ * randomly (delaunay.c:513-522), and callers fall back to nif_mesh_build.
+ * NIF_ERR_CAPACITY where an insertion's cavity exceeds 256 tets.  The tet
+ * buffers hold nif_delaunay_max_tets(n) tets; *info->n_tets are written.
+ * Synchronises `stream` once per insertion round. */
+typedef struct {
+    int64_t n_tets;             /* tets written */
+    int32_t rounds;             /* insertion rounds */
+    int32_t max_cavity;         /* largest cavity (tets) */
+    int64_t exact_evaluations;  /* predicates the error bound could not certify */
+    int32_t tet_slots;          /* slots used before compaction */
+    int32_t error;              /* builder's internal error code, 0 if none */
+    int64_t bad_orientation;    /* check: tets not positively oriented */
+    int64_t bad_adjacency;      /* check: asymmetric neighbour entries */
+    int64_t non_delaunay_faces; /* check: faces whose opposite vertex is inside */
+    int64_t cospherical_faces;  /* check: ... exactly on the circumsphere */
+} nif_delaunay_info;
+int nif_delaunay_max_tets(int n, int *cap);
+int nif_delaunay_workspace_bytes(int n, size_t *bytes);
+int nif_delaunay_build(const double *d_keys, int n, void *d_ws, size_t ws_bytes, double *d_vxyz,
+                       int32_t *d_tet_v, int32_t *d_tet_n, int tet_cap, void *stream,
+                       nif_delaunay_info *info);
+
 typedef struct nif_dmesh nif_dmesh;
 
 /* Size in bytes of the device buffer that holds a resident mesh of
@@ -176,7 +212,8 @@ typedef struct {
     int64_t rows_outside;   /* queries outside the super-simplex (empty rows) */
     int64_t walk_steps;     /* total point-location steps */
     int32_t first_status;   /* status of a failing row, NIF_OK if none */
-    int32_t reserved;
+    int32_t rows_wide;      /* rows whose cavity exceeded a split-row record
+                             * and ran in the fused row kernel (speed only) */
     /* NIF_PRED_AUDIT / NIF_PRED_EXACT meshes, over the tests natinterp3d makes
      * for these rows: walk orientation tests and cavity in-sphere tests whose
      * fast value the error bound cannot certify, and those whose decision the
@@ -258,6 +295,17 @@ int nif_spmm_t(int64_t M, int64_t N, int64_t nnz, const int32_t *d_rowptr, const
                const void *d_vals, int vals_dtype, const void *d_x, int x_dtype, int D, void *d_y,
                int y_dtype, void *d_ws, size_t ws_bytes, void *stream);
 
+/* The same product, the columns processed in the order d_key_rank gives
+ * (d_key_rank[k] = position of column k; a permutation of 0..N-1, such as a
+ * spatial order of the keys, so that neighbouring keys, whose rows overlap,
+ * gather their x rows while they are still in L2).  Results are identical
+ * bit for bit; a d_key_rank that is not a permutation gives unspecified
+ * values but no out-of-range access.  Same workspace as nif_spmm_t. */
+int nif_spmm_t_ordered(int64_t M, int64_t N, int64_t nnz, const int32_t *d_rowptr,
+                       const int32_t *d_cols, const void *d_vals, int vals_dtype, const void *d_x,
+                       int x_dtype, int D, void *d_y, int y_dtype, const int32_t *d_key_rank,
+                       void *d_ws, size_t ws_bytes, void *stream);
+
 /* Gradient of a loss through interpolation with respect to the query
  * positions: gq[i, :] = sum_k (gout[i, :] . values[k, :]) dw_ik/dq_i, from the
  * analytic derivative of every stolen volume (the virtual-tet terms of
@@ -273,6 +321,32 @@ int nif_query_grad(const nif_dmesh *m, const void *d_queries, int query_dtype, i
                    const double *d_row_totals, const void *d_values, int values_dtype, int D,
                    const void *d_gout, int gout_dtype, void *d_gq, void *d_ws, size_t ws_bytes,
                    void *stream, nif_summary *summary);
+
+/* The same gradient without recomputing point location and cavities: the
+ * forward keeps every row's cavity record (its cavity tets in natinterp3d's
+ * visiting order, their face-circumcentre choices and boundary faces;
+ * 1,552 bytes a row, nif_records_bytes) by calling
+ * nif_weights_count_records in place of nif_weights_count, then
+ * nif_weights_fill as usual; nif_query_grad_records then takes that
+ * workspace (unchanged since) and the records, for the same queries, M and
+ * centroid.  Meshes with natinterp3d's fast predicates only (NIF_ERR_ARG
+ * otherwise; nif_query_grad serves the other modes).  d_records must be
+ * 256-byte aligned.  The results equal nif_query_grad's bit for bit.  The
+ * summary counts the gradient's own passes except the large-row kernel's
+ * (whose rows the forward's summary reported).  (natinterp3d has no
+ * counterpart.) */
+int nif_records_bytes(int64_t M, size_t *bytes);
+int nif_weights_count_records(const nif_dmesh *m, const void *d_queries, int query_dtype, int64_t M,
+                              const double centroid[3], void *d_ws, size_t ws_bytes,
+                              int32_t *d_rowptr, void *d_records, size_t records_bytes,
+                              void *stream, nif_summary *summary);
+int nif_query_grad_records(const nif_dmesh *m, const void *d_queries, int query_dtype, int64_t M,
+                           const double centroid[3], const int32_t *d_rowptr,
+                           const double *d_weights, const double *d_row_totals,
+                           const void *d_values, int values_dtype, int D, const void *d_gout,
+                           int gout_dtype, void *d_gq, const void *d_ws, size_t ws_bytes,
+                           void *d_records, size_t records_bytes, void *stream,
+                           nif_summary *summary);
 
 /* ---- batched problems (no counterpart in natinterp3d, which needs one
  * Interpolator and one query call per key set) ------------------------------
@@ -313,9 +387,14 @@ int nif_batch_summary(const nif_dbatch *b, int64_t total_queries, const void *d_
  * waits for the last complete call and returns the device time in
  * milliseconds of {query bucketing, shared-memory row kernel, large-row
  * kernel, CSR scan or epilogue}, averaged over the calls since the last
- * enable or read (at most the last 64).  (natinterp3d has no counterpart.) */
+ * enable or read (at most the last 64).  (natinterp3d has no counterpart.)
+ * nif_profile_kernels then returns, for the same calls, the device time in
+ * milliseconds and the launches per call of each row kernel: {k_locate,
+ * k_rows_cavity, k_rows_volume, k_rows_fast} (events bracket each launch,
+ * at most 48 a call). */
 int nif_profile_enable(int on);
 int nif_profile_read(double ms[4]);
+int nif_profile_kernels(double ms[4], double launches[4]);
 
 /* Measured FP64 throughput of the current device in TFLOP/s (2 flops per
  * multiply-add pair), with fused multiply-add and with separately rounded

@@ -37,7 +37,7 @@ MESH_CFLAGS = ['-std=c11', '-O3', '-fno-math-errno', '-flto', '-fopenmp',
                '-DUSE_LIST_NODE_ALLOCATOR', '-fvisibility=hidden']
 MESH_LDFLAGS = ['-fopenmp', '-flto', '-lm', '-lpthread']
 
-CUDA_SOURCES = ['nif_cuda.cu']
+CUDA_SOURCES = ['nif_cuda.cu', 'nif_delaunay.cu']
 NVCC_FLAGS = ['-O3', '-std=c++17', '-gencode', 'arch=compute_100a,code=sm_100a', '-lineinfo',
               '-fmad=false', '--prec-div=true', '--prec-sqrt=true', '-Xcompiler', '-fPIC',
               '-Xcompiler', '-fvisibility=hidden', '-cudart', 'static', '--expt-relaxed-constexpr']

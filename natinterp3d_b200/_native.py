@@ -160,12 +160,12 @@ class Summary(ctypes.Structure):
     _fields_ = [('nnz', ctypes.c_int64), ('rows_large', ctypes.c_int64),
                 ('rows_failed', ctypes.c_int64), ('rows_outside', ctypes.c_int64),
                 ('walk_steps', ctypes.c_int64), ('first_status', ctypes.c_int32),
-                ('reserved', ctypes.c_int32), ('orient_uncertain', ctypes.c_int64),
+                ('rows_wide', ctypes.c_int32), ('orient_uncertain', ctypes.c_int64),
                 ('orient_flipped', ctypes.c_int64), ('insphere_uncertain', ctypes.c_int64),
                 ('insphere_flipped', ctypes.c_int64)]
 
     def as_dict(self):
-        return {k: getattr(self, k) for k, _ in self._fields_ if k != 'reserved'}
+        return {k: getattr(self, k) for k, _ in self._fields_}
 
     @classmethod
     def from_dict(cls, d):
@@ -174,6 +174,18 @@ class Summary(ctypes.Structure):
             if k in d:
                 setattr(s, k, int(d[k]))
         return s
+
+
+class DelaunayInfo(ctypes.Structure):
+    """nif_delaunay_info: outcome and exact checks of a GPU construction."""
+    _fields_ = [('n_tets', ctypes.c_int64), ('rounds', ctypes.c_int32),
+                ('max_cavity', ctypes.c_int32), ('exact_evaluations', ctypes.c_int64),
+                ('tet_slots', ctypes.c_int32), ('error', ctypes.c_int32),
+                ('bad_orientation', ctypes.c_int64), ('bad_adjacency', ctypes.c_int64),
+                ('non_delaunay_faces', ctypes.c_int64), ('cospherical_faces', ctypes.c_int64)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
 
 
 class Tuning(ctypes.Structure):
@@ -210,6 +222,7 @@ CUDA_SIGNATURES = {
                                 ctypes.POINTER(Summary)]),
     'nif_profile_enable': (c_int, [c_int]),
     'nif_profile_read': (c_int, [c_double_p]),
+    'nif_profile_kernels': (c_int, [c_double_p, c_double_p]),
     'nif_measure_fp64_peak': (c_int, [c_double_p, c_double_p]),
     'nif_query_summary': (c_int, [c_void_p, c_int64, c_int, c_void_p, c_size_t, c_void_p,
                                   ctypes.POINTER(Summary)]),
@@ -218,9 +231,24 @@ CUDA_SIGNATURES = {
     'nif_spmm_t_workspace_bytes': (c_int, [c_int64, c_int64, c_int64, ctypes.POINTER(c_size_t)]),
     'nif_spmm_t': (c_int, [c_int64, c_int64, c_int64, c_void_p, c_void_p, c_void_p, c_int, c_void_p,
                            c_int, c_int, c_void_p, c_int, c_void_p, c_size_t, c_void_p]),
+    'nif_spmm_t_ordered': (c_int, [c_int64, c_int64, c_int64, c_void_p, c_void_p, c_void_p, c_int,
+                                   c_void_p, c_int, c_int, c_void_p, c_int, c_void_p, c_void_p,
+                                   c_size_t, c_void_p]),
     'nif_query_grad': (c_int, [c_void_p, c_void_p, c_int, c_int64, c_double_p, c_void_p, c_void_p,
                                c_void_p, c_void_p, c_int, c_int, c_void_p, c_int, c_void_p,
                                c_void_p, c_size_t, c_void_p, ctypes.POINTER(Summary)]),
+    'nif_records_bytes': (c_int, [c_int64, ctypes.POINTER(c_size_t)]),
+    'nif_delaunay_max_tets': (c_int, [c_int, ctypes.POINTER(c_int)]),
+    'nif_delaunay_workspace_bytes': (c_int, [c_int, ctypes.POINTER(c_size_t)]),
+    'nif_delaunay_build': (c_int, [c_void_p, c_int, c_void_p, c_size_t, c_void_p, c_void_p, c_void_p,
+                                   c_int, c_void_p, ctypes.POINTER(DelaunayInfo)]),
+    'nif_weights_count_records': (c_int, [c_void_p, c_void_p, c_int, c_int64, c_double_p, c_void_p,
+                                          c_size_t, c_void_p, c_void_p, c_size_t, c_void_p,
+                                          ctypes.POINTER(Summary)]),
+    'nif_query_grad_records': (c_int, [c_void_p, c_void_p, c_int, c_int64, c_double_p, c_void_p,
+                                       c_void_p, c_void_p, c_void_p, c_int, c_int, c_void_p, c_int,
+                                       c_void_p, c_void_p, c_size_t, c_void_p, c_size_t, c_void_p,
+                                       ctypes.POINTER(Summary)]),
     'nif_batch_bytes': (c_int, [c_int, ctypes.POINTER(c_size_t)]),
     'nif_batch_create': (c_int, [c_int, ctypes.POINTER(c_void_p), c_void_p, c_size_t, c_void_p,
                                  ctypes.POINTER(c_void_p)]),

@@ -6,9 +6,12 @@ and back-propagates into both arguments:
 * d/dvalues = W^T @ grad_out, a deterministic transpose product (CSC built by
   a stable sort on the GPU, no floating-point atomics);
 * d/dqueries from the analytic derivative of the Sibson coordinates with
-  respect to the query position (the GPU kernel recomputes each query's
-  cavity and differentiates the virtual-tet volumes, the only terms that
-  move with the query).
+  respect to the query position (the GPU kernel differentiates the
+  virtual-tet volumes, the only terms that move with the query).  The
+  forward keeps every row's cavity record (1,552 bytes a row) so that the
+  backward starts from it; beyond RECORDS_MAX_BYTES of records, or on meshes
+  with other than the default fast predicates, the backward locates and
+  floods each query's cavity again (same results, bit for bit).
 
 The weights are computed in float64 on the device and cast to the query dtype;
 the product and the output use the promoted dtype of (queries, values).  Rows
@@ -23,6 +26,9 @@ import torch
 
 __all__ = ['interpolate', 'SibsonInterpolation']
 
+# largest record buffer the forward keeps for the backward (bytes)
+RECORDS_MAX_BYTES = 16 << 30
+
 
 class _SibsonFn(torch.autograd.Function):
     @staticmethod
@@ -30,8 +36,12 @@ class _SibsonFn(torch.autograd.Function):
         dm = interp.device_mesh
         q = queries.detach().contiguous()
         v = values.detach()
-        rowptr, cols, w64, totals = dm.weights_csr(q, interp.centroid, vals_dtype=torch.float64,
-                                                   return_totals=True)
+        keep = (queries.requires_grad and dm.predicates == 'fast'
+                and dm.records_bytes(q.shape[0]) <= RECORDS_MAX_BYTES)
+        res = dm.weights_csr(q, interp.centroid, vals_dtype=torch.float64, return_totals=True,
+                             keep_records=keep)
+        rowptr, cols, w64, totals = res[:4]
+        ctx.records = res[4] if keep else None
         # weights take the query dtype (as get_weights does); the product uses
         # the promoted dtype of (weights, values), summed in stored column order
         vals = w64.to(q.dtype)
@@ -48,7 +58,9 @@ class _SibsonFn(torch.autograd.Function):
         g = grad_out.contiguous()
         gq = gv = None
         if ctx.needs_input_grad[0]:
-            gq = dm.query_grad(q, v, g, ctx.interp.centroid, rowptr, w64, totals)
+            gq = dm.query_grad(q, v, g, ctx.interp.centroid, rowptr, w64, totals,
+                               records=ctx.records)
+        ctx.records = None
         if ctx.needs_input_grad[1]:
             gv = dm.spmm_t(rowptr, cols, vals, g.reshape(q.shape[0], -1), dm.n_keys)
             gv = gv.reshape(ctx.value_shape).to(v.dtype)

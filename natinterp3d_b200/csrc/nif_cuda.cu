@@ -773,16 +773,33 @@ __global__ void k_spmm(int64_t M, int D, const int32_t *__restrict__ rowptr,
     }
 }
 
+// sort key of entry e: its column, or the column's rank in a caller-given
+// processing order (clamped to [0, N) so that a bad rank cannot leave the sort's range)
 __global__ void k_row_of(int64_t M, const int32_t *__restrict__ rowptr, int32_t *__restrict__ rowof,
                          uint32_t *__restrict__ keys, const int32_t *__restrict__ cols,
-                         int32_t *__restrict__ idx) {
+                         int32_t *__restrict__ idx, const int32_t *__restrict__ rank, int64_t N) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < M;
          i += (int64_t)gridDim.x * blockDim.x)
         for (int e = rowptr[i]; e < rowptr[i + 1]; e++) {
             rowof[e] = (int32_t)i;
-            keys[e] = (uint32_t)cols[e];
+            int k = cols[e];
+            if (rank) {
+                k = rank[k];
+                k = k < 0 ? 0 : (k >= N ? (int)(N - 1) : k);
+            }
+            keys[e] = (uint32_t)k;
             idx[e] = e;
         }
+}
+
+// inverse of a processing order: inv[rank[k]] = k (entries a bad rank leaves
+// unset stay -1 and are skipped)
+__global__ void k_rank_inverse(int64_t N, const int32_t *__restrict__ rank, int32_t *__restrict__ inv) {
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < N;
+         k += (int64_t)gridDim.x * blockDim.x) {
+        const int r = rank[k];
+        if (r >= 0 && r < N) inv[r] = (int32_t)k;
+    }
 }
 
 // stable LSD radix sort of (key, value) pairs, 4 bits per pass
@@ -901,14 +918,19 @@ __global__ void k_colptr(const uint32_t *__restrict__ keys, int64_t n, int64_t N
 template <class WT, class XT, class CT>
 __global__ void k_spmm_t(int64_t N, int D, const int32_t *__restrict__ colptr,
                          const int32_t *__restrict__ perm, const int32_t *__restrict__ rowof,
-                         const WT *__restrict__ vals, const XT *__restrict__ x, CT *__restrict__ y) {
+                         const WT *__restrict__ vals, const XT *__restrict__ x, CT *__restrict__ y,
+                         const int32_t *__restrict__ inv) {
     for (int64_t u = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; u < N * D;
          u += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t k = u / D;
-        const int d = (int)(u - k * D);
+        // position r of the processing order: column k (keys in the caller's
+        // order, or inv[r] for a caller-given order)
+        const int64_t r = u / D;
+        const int d = (int)(u - r * D);
+        const int64_t k = inv ? (int64_t)inv[r] : r;
+        if (k < 0 || k >= N) continue;
         CT acc = (CT)0;
-        int p = colptr[k];
-        const int p1 = colptr[k + 1];
+        int p = colptr[r];
+        const int p1 = colptr[r + 1];
         // four entries' loads issued together; the sum stays in ascending row order
         for (; p + 4 <= p1; p += 4) {
             const int e0 = perm[p], e1 = perm[p + 1], e2 = perm[p + 2], e3 = perm[p + 3];
@@ -925,7 +947,7 @@ __global__ void k_spmm_t(int64_t N, int D, const int32_t *__restrict__ colptr,
             const int e = perm[p];
             acc = Arith<CT>::add(acc, Arith<CT>::mul((CT)vals[e], (CT)x[(int64_t)rowof[e] * D + d]));
         }
-        y[u] = acc;
+        y[k * D + d] = acc;
     }
 }
 
@@ -1057,10 +1079,11 @@ __global__ void __launch_bounds__(FAST_BLOCK, OCC) k_rows_fast(MeshView M, const
     if (g.lane == 0 && steps) atomicAdd(&sum->walk_steps, steps);
 }
 
-// Point location of every row (natinterp3d's signs): one warp per row, rows
-// in bucket order as the row kernels take them; located[i] = the tet, -1
-// outside the super-simplex, -2 a walk that hit its step limit.
-template <class QT, class Rows>
+// Point location of every row: one warp per row, rows in bucket order as
+// the row kernels take them; located[i] = the tet, -1 outside the
+// super-simplex, -2 a walk that hit its step limit, -3 (PM_FILTER) a walk
+// test the error bound cannot certify (the large kernel resolves the row).
+template <class QT, class Rows, int PM = PM_PLAIN>
 __global__ void __launch_bounds__(FAST_BLOCK) k_locate(const __grid_constant__ Rows rows,
                                                        const QT *__restrict__ Q,
                                                        const int *__restrict__ order, int64_t nrows,
@@ -1092,9 +1115,11 @@ __global__ void __launch_bounds__(FAST_BLOCK) k_locate(const __grid_constant__ R
         const dv3 q = load_query(Q, i, cen);
         RowInfo r{ST_OK, 0, 0, false, false, 0.0, 0, 0, 0, 0, 0};
         bool on_face = false;
-        const int t = locate<G, PM_PLAIN>(M, q, g, scr, r, on_face);
+        const int t = locate<G, PM>(M, q, g, scr, r, on_face);
         steps += r.steps;
-        if (g.lane == 0) located[i] = r.status != ST_OK ? -2 : (r.outside ? -1 : t);
+        if (g.lane == 0)
+            located[i] = r.status == ST_UNCERTAIN ? -3
+                         : (r.status != ST_OK ? -2 : (r.outside ? -1 : t));
         g.sync();
         s += tile <= 0 ? ng : 1;
     }
@@ -1107,7 +1132,7 @@ __global__ void __launch_bounds__(FAST_BLOCK) k_locate(const __grid_constant__ R
 // belongs to position s.  Each kernel holds one half of the row code.
 // Rows whose cavity fits the shared-memory capacities but not a record are
 // queued in `wide` for the fused row kernel, larger ones for the large kernel.
-template <class QT, class Rows, int OCC>
+template <class QT, class Rows, int OCC, int PM = PM_PLAIN>
 __global__ void __launch_bounds__(FAST_BLOCK, OCC)
     k_rows_cavity(const __grid_constant__ Rows rows, const QT *__restrict__ Q,
                   const int *__restrict__ order, int64_t nrows, const int *__restrict__ located,
@@ -1137,13 +1162,16 @@ __global__ void __launch_bounds__(FAST_BLOCK, OCC)
         RowHead h{0, t, RS_OK, 0};
         if (t == -1) {
             h.state = RS_OUTSIDE;
+        } else if (t == -3) {
+            h.state = RS_QUEUED;
+            if (g.lane == 0) lq.list[atomicAdd(&sum->large_count, 1)] = (int)i;
         } else if (t < 0) {
             h.state = RS_WALK;
         } else {
             const double *cen;
             const MeshView &M = rows.get(i, cur, &sview[threadIdx.x / G], g, cen);
             const dv3 q = load_query(Q, i, cen);
-            const int rc = cavity_record<G>(M, q, ws, g, t, h, ents + s * REC_CAV);
+            const int rc = cavity_record<G, CavWS, PM>(M, q, ws, g, t, h, ents + s * REC_CAV);
             if (rc != REC_DONE) {
                 h.state = RS_QUEUED;
                 if (g.lane == 0) {
@@ -1514,6 +1542,32 @@ QueryLayout carve_query(Carve &c, int64_t M, int mode) {
     return L;
 }
 
+// Split-row records of every row of a get_weights call, kept for the
+// gradient of the same rows (nif_weights_count_records /
+// nif_query_grad_records), and the gradient pass's own scratch: rows it
+// would queue again are already in the forward's queues, so its re-queues
+// go to `requeue` and are dropped.
+struct RecordLayout {
+    RowHead *heads;          // [M], record of bucket position s at s
+    RowEntry *ents;          // [M * REC_CAV]
+    DevSummary *sum;         // counters of the gradient's record and wide passes
+    DevSummary *large_sum;   // the forward's counters: the large pass's queue length
+    int *requeue;            // [M]
+    unsigned long long *counter;
+};
+
+RecordLayout carve_records(Carve &c, int64_t M) {
+    RecordLayout R{};
+    const int64_t m1 = M > 0 ? M : 1;
+    R.heads = c.take<RowHead>(m1);
+    R.ents = c.take<RowEntry>(m1 * REC_CAV);
+    R.sum = c.take<DevSummary>(1);
+    R.large_sum = c.take<DevSummary>(1);
+    R.requeue = c.take<int>(m1);
+    R.counter = c.take<unsigned long long>(1);
+    return R;
+}
+
 template <class OutT>
 void launch_scan(const int *in, int64_t n, OutT *bsum, OutT *total, OutT *out, cudaStream_t st) {
     const int64_t nb = (n + SCAN_TILE - 1) / SCAN_TILE;
@@ -1558,31 +1612,58 @@ int resident_blocks(Kern k, int threads, size_t smem) {
 // set per call in a ring of PROF_RING sets, so that timed loops never wait
 // on the host; nif_profile_read averages the calls recorded since the last
 // enable or read.
+// Within the row phase, events also bracket each launch of the row kernels
+// (kernel spans, by kind), so that the time of one kernel is known apart
+// from the others.
 constexpr int PROF_EVENTS = 5;  // start | bucketing | fast rows | large rows | finish
 constexpr int PROF_RING = 64;
+constexpr int PROF_SPANS = 48;  // kernel spans recorded per call (further launches are not)
+constexpr int PROF_KINDS = 4;   // k_locate | k_rows_cavity | k_rows_volume | k_rows_fast
+enum { SPAN_LOCATE = 0, SPAN_CAVITY = 1, SPAN_VOLUME = 2, SPAN_FUSED = 3 };
 struct Profiler {
     bool on = false;
     bool created = false;
     int calls = 0;     // calls started since enable / read (the ring keeps the last PROF_RING)
     int marks = 0;     // marks of the current call
     cudaEvent_t ev[PROF_RING][PROF_EVENTS];
+    cudaEvent_t sev[PROF_RING][PROF_SPANS][2];
+    int skind[PROF_RING][PROF_SPANS];
+    int nspan[PROF_RING];
+    // per-kind averages of the calls the last nif_profile_read covered
+    double kms[PROF_KINDS], klaunch[PROF_KINDS];
 };
 Profiler g_prof;
 
 inline void prof_mark(int k, cudaStream_t st) {
     if (!g_prof.on) return;
     if (!g_prof.created) {
-        for (int r = 0; r < PROF_RING; r++)
+        for (int r = 0; r < PROF_RING; r++) {
             for (int i = 0; i < PROF_EVENTS; i++) cudaEventCreate(&g_prof.ev[r][i]);
+            for (int i = 0; i < PROF_SPANS; i++) {
+                cudaEventCreate(&g_prof.sev[r][i][0]);
+                cudaEventCreate(&g_prof.sev[r][i][1]);
+            }
+        }
         g_prof.created = true;
     }
     if (k == 0) {
         g_prof.calls++;
         g_prof.marks = 0;
+        g_prof.nspan[(g_prof.calls - 1) % PROF_RING] = 0;
     }
     if (g_prof.calls == 0) return;
     cudaEventRecord(g_prof.ev[(g_prof.calls - 1) % PROF_RING][k], st);
     g_prof.marks = k + 1;
+}
+
+// brackets one row-kernel launch of the current call (begin: end = false)
+inline void prof_span(int kind, bool end, cudaStream_t st) {
+    if (!g_prof.on || !g_prof.created || g_prof.calls == 0 || g_prof.marks != 2) return;
+    const int r = (g_prof.calls - 1) % PROF_RING;
+    int &n = g_prof.nspan[r];
+    if (n >= PROF_SPANS) return;
+    cudaEventRecord(g_prof.sev[r][n][end ? 1 : 0], st);
+    if (end) g_prof.skind[r][n++] = kind;
 }
 
 // bucket the queries (writes L.order); positions fit int32 because M < 2^31
@@ -1699,22 +1780,33 @@ constexpr int sink_occ() {
 // their meshes: k_locate over all rows, then per chunk of REC_CHUNK rows the
 // cavity records and the volumes.  Rows whose cavity exceeds a record are
 // left in `wide` (count in R.sum->wide_count) for the fused kernel.
-template <class QT, class Rows, class Sink, int OCC>
+template <class QT, class Rows, class Sink, int OCC, int PM = PM_PLAIN>
 void launch_split(const Launch &lc, const Rows &rows, const QT *Q, int64_t M, const RowSet &R,
-                  RowHead *heads, RowEntry *ents, int *wide, const Sink &sink, cudaStream_t st) {
+                  RowHead *heads, RowEntry *ents, int *wide, const Sink &sink, cudaStream_t st,
+                  bool keep = false) {
     constexpr int GPB = FAST_BLOCK / FAST_G;
     constexpr int COCC = NIF_CAV_OCC > 0 ? NIF_CAV_OCC : OCC;
     constexpr int VOCC = sink_occ<Sink, (NIF_VOL_OCC > 0 ? NIF_VOL_OCC : OCC)>();
     int *located = const_cast<int *>(R.located);
-    launch_rows(k_locate<QT, Rows>, lc, M, 0, R.counter, st, rows, Q, R.order, M, located, R.sum);
+    prof_span(SPAN_LOCATE, false, st);
+    launch_rows(k_locate<QT, Rows, PM>, lc, M, 0, R.counter, st, rows, Q, R.order, M, located,
+                R.sum);
+    prof_span(SPAN_LOCATE, true, st);
     for (int64_t c0 = 0; c0 < M; c0 += REC_CHUNK) {
         const int64_t n = min((int64_t)REC_CHUNK, M - c0);
-        launch_rows(k_rows_cavity<QT, Rows, COCC>, lc, n, GPB * sizeof(CavWS), R.counter, st, rows, Q,
-                    R.order + c0, n, (const int *)located, heads, ents, wide, LargeQueue{R.large},
+        // one chunk's records, or (keep) every row's at its own position
+        RowHead *h = keep ? heads + c0 : heads;
+        RowEntry *e = keep ? ents + c0 * REC_CAV : ents;
+        prof_span(SPAN_CAVITY, false, st);
+        launch_rows(k_rows_cavity<QT, Rows, COCC, PM>, lc, n, GPB * sizeof(CavWS), R.counter, st,
+                    rows, Q, R.order + c0, n, (const int *)located, h, e, wide, LargeQueue{R.large},
                     R.sum);
+        prof_span(SPAN_CAVITY, true, st);
+        prof_span(SPAN_VOLUME, false, st);
         launch_rows(k_rows_volume<QT, Rows, Sink, VOCC>, lc, n, GPB * sizeof(VolWS), R.counter, st,
-                    rows, Q, R.order + c0, n, (const RowHead *)heads, (const RowEntry *)ents, sink,
+                    rows, Q, R.order + c0, n, (const RowHead *)h, (const RowEntry *)e, sink,
                     LargeQueue{R.large}, R.sum);
+        prof_span(SPAN_VOLUME, true, st);
     }
 }
 
@@ -1725,34 +1817,45 @@ void launch_split(const Launch &lc, const Rows &rows, const QT *Q, int64_t M, co
 template <class QT, class Sink, int PM>
 void launch_fast(const nif_dmesh *m, const QT *Q, int64_t M, const Centroid &cen,
                  const RowSet &R, const Sink &sink, cudaStream_t st, RowHead *heads = nullptr,
-                 RowEntry *ents = nullptr, int *wide = nullptr) {
-    if constexpr (PM == PM_PLAIN) {
+                 RowEntry *ents = nullptr, int *wide = nullptr, bool keep = false) {
+    if constexpr (PM == PM_PLAIN || PM == PM_FILTER) {
         if (R.located && heads && !R.nrows_dev) {
             const Launch lc{m->tune.tile, m->num_sms};
             const OneMesh rows{m->view, cen};
             if (m->tune.blocks_per_sm == OCC_LO)
-                launch_split<QT, OneMesh, Sink, OCC_LO>(lc, rows, Q, M, R, heads, ents, wide, sink, st);
+                launch_split<QT, OneMesh, Sink, OCC_LO, PM>(lc, rows, Q, M, R, heads, ents, wide, sink,
+                                                            st, keep);
             else
-                launch_split<QT, OneMesh, Sink, OCC_HI>(lc, rows, Q, M, R, heads, ents, wide, sink, st);
+                launch_split<QT, OneMesh, Sink, OCC_HI, PM>(lc, rows, Q, M, R, heads, ents, wide, sink,
+                                                            st, keep);
             // rows whose cavity exceeds a record: the fused row kernel (which
             // queues what exceeds its own capacities for the large kernel)
             const RowSet W{wide, &R.sum->wide_count, R.large, R.sum, R.counter, nullptr};
-            launch_fast_loc<QT, Sink, PM_PLAIN>(m, Q, M, cen, W, sink, st);
+            prof_span(SPAN_FUSED, false, st);
+            launch_fast_loc<QT, Sink, PM>(m, Q, M, cen, W, sink, st);
+            prof_span(SPAN_FUSED, true, st);
             return;
         }
     }
+    prof_span(SPAN_FUSED, false, st);
     launch_fast_loc<QT, Sink, PM>(m, Q, M, cen, R, sink, st);
+    prof_span(SPAN_FUSED, true, st);
 }
 
 // fast rows (filtered when the mesh's predicate mode is not the default),
-// then the rows they queued; large_groups workspaces in L
+// then the rows they queued; large_groups workspaces in L.  With rec, every
+// row's split-row record is kept there (natinterp3d's signs only).
 template <class QT, class Sink>
 void run_rows(const nif_dmesh *m, const QT *Q, int64_t M, const Centroid &cen, const QueryLayout &L,
-              const Sink &sink, cudaStream_t st, int large_groups = LARGE_GROUPS) {
-    if (m->view.pmode == PRED_FAST)
+              const Sink &sink, cudaStream_t st, int large_groups = LARGE_GROUPS,
+              const RecordLayout *rec = nullptr) {
+    if (m->view.pmode == PRED_FAST && rec)
+        launch_fast<QT, Sink, PM_PLAIN>(m, Q, M, cen, all_rows(L), sink, st, rec->heads, rec->ents,
+                                        L.wide, true);
+    else if (m->view.pmode == PRED_FAST)
         launch_fast<QT, Sink, PM_PLAIN>(m, Q, M, cen, all_rows(L), sink, st, L.heads, L.ents, L.wide);
     else
-        launch_fast<QT, Sink, PM_FILTER>(m, Q, M, cen, all_rows(L), sink, st);
+        launch_fast<QT, Sink, PM_FILTER>(m, Q, M, cen, all_rows(L), sink, st, L.heads, L.ents, L.wide);
     prof_mark(2, st);
     k_rows_large<QT, Sink><<<large_groups, 32, 0, st>>>(m->view, Q, cen, LargeQueue{L.large_list},
                                                         sink, L.large_ws, L.exact, L.sum);
@@ -1799,7 +1902,7 @@ int read_summary(const QueryLayout &L, cudaStream_t st, nif_summary *out, int64_
         out->rows_outside = (int64_t)d.rows_outside;
         out->walk_steps = (int64_t)d.walk_steps;
         out->first_status = d.first_status;
-        out->reserved = 0;
+        out->rows_wide = d.wide_count;
         out->orient_uncertain = (int64_t)d.orient_unc;
         out->orient_flipped = (int64_t)d.orient_flip;
         out->insphere_uncertain = (int64_t)d.insphere_unc;
@@ -2118,9 +2221,18 @@ NIF_EXPORT int nif_query_workspace_bytes(const nif_dmesh *m, int64_t M, int mode
     return NIF_OK;
 }
 
-NIF_EXPORT int nif_weights_count(const nif_dmesh *m, const void *d_queries, int query_dtype,
-                                 int64_t M, const double centroid[3], void *d_ws, size_t ws_bytes,
-                                 int32_t *d_rowptr, void *stream, nif_summary *summary) {
+NIF_EXPORT int nif_records_bytes(int64_t M, size_t *bytes) {
+    if (!bytes || M < 0) return NIF_ERR_ARG;
+    Carve c{nullptr, 0, (size_t)-1, true};
+    carve_records(c, M);
+    *bytes = align_up(c.off, 256);
+    return NIF_OK;
+}
+
+namespace {
+int weights_count(const nif_dmesh *m, const void *d_queries, int query_dtype, int64_t M,
+                  const double centroid[3], void *d_ws, size_t ws_bytes, int32_t *d_rowptr,
+                  const RecordLayout *rec, void *stream, nif_summary *summary) {
     int rc = check_query_args(m, d_queries, query_dtype, M, centroid, d_ws);
     if (rc != NIF_OK) return rc;
     if (!d_rowptr) return NIF_ERR_ARG;
@@ -2136,10 +2248,10 @@ NIF_EXPORT int nif_weights_count(const nif_dmesh *m, const void *d_queries, int 
         StageSink sink{L.cnt, L.staged, L.scols, L.svals, L.refill, L.sum, L.rtot};
         if (query_dtype == NIF_F64) {
             run_bucketing(m, static_cast<const double *>(d_queries), M, cen, L, st);
-            run_rows(m, static_cast<const double *>(d_queries), M, cen, L, sink, st);
+            run_rows(m, static_cast<const double *>(d_queries), M, cen, L, sink, st, LARGE_GROUPS, rec);
         } else {
             run_bucketing(m, static_cast<const float *>(d_queries), M, cen, L, st);
-            run_rows(m, static_cast<const float *>(d_queries), M, cen, L, sink, st);
+            run_rows(m, static_cast<const float *>(d_queries), M, cen, L, sink, st, LARGE_GROUPS, rec);
         }
     }
     launch_scan<int64_t>(L.cnt, M, L.scan_bsum, L.scan_total, L.off64, st);
@@ -2151,6 +2263,29 @@ NIF_EXPORT int nif_weights_count(const nif_dmesh *m, const void *d_queries, int 
     if (rc != NIF_OK) return rc;
     if (total > (int64_t)INT32_MAX) return NIF_ERR_OVERFLOW;
     return NIF_OK;
+}
+}  // namespace
+
+NIF_EXPORT int nif_weights_count(const nif_dmesh *m, const void *d_queries, int query_dtype,
+                                 int64_t M, const double centroid[3], void *d_ws, size_t ws_bytes,
+                                 int32_t *d_rowptr, void *stream, nif_summary *summary) {
+    return weights_count(m, d_queries, query_dtype, M, centroid, d_ws, ws_bytes, d_rowptr, nullptr,
+                         stream, summary);
+}
+
+NIF_EXPORT int nif_weights_count_records(const nif_dmesh *m, const void *d_queries, int query_dtype,
+                                         int64_t M, const double centroid[3], void *d_ws,
+                                         size_t ws_bytes, int32_t *d_rowptr, void *d_records,
+                                         size_t records_bytes, void *stream, nif_summary *summary) {
+    if (!m || m->view.pmode != PRED_FAST || !d_records) return NIF_ERR_ARG;
+    if (reinterpret_cast<uintptr_t>(d_records) % 256 != 0) return NIF_ERR_ARG;
+    size_t need = 0;
+    if (nif_records_bytes(M, &need) != NIF_OK) return NIF_ERR_ARG;
+    if (records_bytes < need) return NIF_ERR_WORKSPACE;
+    Carve c{static_cast<unsigned char *>(d_records), 0, records_bytes, true};
+    const RecordLayout R = carve_records(c, M);
+    return weights_count(m, d_queries, query_dtype, M, centroid, d_ws, ws_bytes, d_rowptr, &R,
+                         stream, summary);
 }
 
 namespace {
@@ -2261,15 +2396,33 @@ NIF_EXPORT int nif_profile_read(double ms[4]) {
     const int first = last - PROF_RING + 1 > 1 ? last - PROF_RING + 1 : 1;
     if (!g_prof.created || last < 1) return NIF_ERR_ARG;
     NIF_CUDA(cudaEventSynchronize(g_prof.ev[(last - 1) % PROF_RING][PROF_EVENTS - 1]));
-    for (int c = first; c <= last; c++)
+    const int ncalls = last - first + 1;
+    for (int k = 0; k < PROF_KINDS; k++) g_prof.kms[k] = g_prof.klaunch[k] = 0.0;
+    for (int c = first; c <= last; c++) {
+        const int r = (c - 1) % PROF_RING;
         for (int i = 0; i < 4; i++) {
             float t = 0.f;
-            NIF_CUDA(cudaEventElapsedTime(&t, g_prof.ev[(c - 1) % PROF_RING][i],
-                                          g_prof.ev[(c - 1) % PROF_RING][i + 1]));
-            ms[i] += t / (last - first + 1);
+            NIF_CUDA(cudaEventElapsedTime(&t, g_prof.ev[r][i], g_prof.ev[r][i + 1]));
+            ms[i] += t / ncalls;
         }
+        for (int j = 0; j < g_prof.nspan[r]; j++) {
+            float t = 0.f;
+            NIF_CUDA(cudaEventElapsedTime(&t, g_prof.sev[r][j][0], g_prof.sev[r][j][1]));
+            g_prof.kms[g_prof.skind[r][j]] += t / ncalls;
+            g_prof.klaunch[g_prof.skind[r][j]] += 1.0 / ncalls;
+        }
+    }
     g_prof.calls = 0;
     g_prof.marks = 0;
+    return NIF_OK;
+}
+
+NIF_EXPORT int nif_profile_kernels(double ms[4], double launches[4]) {
+    if (!ms || !launches) return NIF_ERR_ARG;
+    for (int k = 0; k < PROF_KINDS; k++) {
+        ms[k] = g_prof.kms[k];
+        launches[k] = g_prof.klaunch[k];
+    }
     return NIF_OK;
 }
 
@@ -2454,19 +2607,19 @@ int spmm_typed(int64_t M, int D, const int32_t *rowptr, const int32_t *cols, con
 
 template <class WT, class XT>
 int spmm_t_typed(int64_t N, int D, const int32_t *colptr, const int32_t *perm, const int32_t *rowof,
-                 const void *vals, const void *x, void *y, cudaStream_t st) {
+                 const void *vals, const void *x, void *y, const int32_t *inv, cudaStream_t st) {
     using CT = typename std::conditional<(sizeof(WT) == 8 || sizeof(XT) == 8), double, float>::type;
     if (N * D == 0) return NIF_OK;
     k_spmm_t<WT, XT, CT><<<blocks_for(N * D, 256), 256, 0, st>>>(
         N, D, colptr, perm, rowof, static_cast<const WT *>(vals), static_cast<const XT *>(x),
-        static_cast<CT *>(y));
+        static_cast<CT *>(y), inv);
     return cuda_rc(cudaGetLastError());
 }
 
 int expect_promoted(int a, int b) { return (a == NIF_F32 && b == NIF_F32) ? NIF_F32 : NIF_F64; }
 
 struct CscLayout {
-    int32_t *rowof, *idx_a, *idx_b, *colptr;
+    int32_t *rowof, *idx_a, *idx_b, *colptr, *inv;
     uint32_t *key_a, *key_b;
     int *hist, *off, *bsum, *total;
 };
@@ -2481,6 +2634,7 @@ CscLayout carve_csc(Carve &c, int64_t nnz, int64_t N) {
     L.key_a = c.take<uint32_t>(nnz > 0 ? nnz : 1);
     L.key_b = c.take<uint32_t>(nnz > 0 ? nnz : 1);
     L.colptr = c.take<int32_t>(N + 1);
+    L.inv = c.take<int32_t>(N > 0 ? N : 1);
     L.hist = c.take<int>(nh);
     L.off = c.take<int>(nh);
     L.bsum = c.take<int>((nh + SCAN_TILE - 1) / SCAN_TILE + 1);
@@ -2517,10 +2671,10 @@ NIF_EXPORT int nif_spmm_t_workspace_bytes(int64_t M, int64_t N, int64_t nnz, siz
     return NIF_OK;
 }
 
-NIF_EXPORT int nif_spmm_t(int64_t M, int64_t N, int64_t nnz, const int32_t *d_rowptr,
-                          const int32_t *d_cols, const void *d_vals, int vals_dtype, const void *d_x,
-                          int x_dtype, int D, void *d_y, int y_dtype, void *d_ws, size_t ws_bytes,
-                          void *stream) {
+namespace {
+int spmm_t_impl(int64_t M, int64_t N, int64_t nnz, const int32_t *d_rowptr, const int32_t *d_cols,
+                const void *d_vals, int vals_dtype, const void *d_x, int x_dtype, int D, void *d_y,
+                int y_dtype, const int32_t *d_key_rank, void *d_ws, size_t ws_bytes, void *stream) {
     size_t need = 0;
     int rc = nif_spmm_t_workspace_bytes(M, N, nnz, &need);
     if (rc != NIF_OK) return rc;
@@ -2535,7 +2689,14 @@ NIF_EXPORT int nif_spmm_t(int64_t M, int64_t N, int64_t nnz, const int32_t *d_ro
     Carve c{reinterpret_cast<unsigned char *>(d_ws), 0, ws_bytes, true};
     CscLayout L = carve_csc(c, nnz, N);
     if (M > 0)
-        k_row_of<<<blocks_for(M, 256), 256, 0, st>>>(M, d_rowptr, L.rowof, L.key_a, d_cols, L.idx_a);
+        k_row_of<<<blocks_for(M, 256), 256, 0, st>>>(M, d_rowptr, L.rowof, L.key_a, d_cols, L.idx_a,
+                                                      d_key_rank, N);
+    const int32_t *inv = nullptr;
+    if (d_key_rank && N > 0) {
+        NIF_CUDA(cudaMemsetAsync(L.inv, 0xff, sizeof(int32_t) * N, st));
+        k_rank_inverse<<<blocks_for(N, 256), 256, 0, st>>>(N, d_key_rank, L.inv);
+        inv = L.inv;
+    }
     // stable sort by column over as many 4-bit digits as the column count needs
     int bits = 0;
     while (bits < 32 && ((int64_t)1 << bits) < N) bits++;
@@ -2554,12 +2715,31 @@ NIF_EXPORT int nif_spmm_t(int64_t M, int64_t N, int64_t nnz, const int32_t *d_ro
     }
     k_colptr<<<blocks_for(N + 1, 256), 256, 0, st>>>(kin, nnz, N, L.colptr);
     if (vals_dtype == NIF_F64 && x_dtype == NIF_F64)
-        return spmm_t_typed<double, double>(N, D, L.colptr, vin, L.rowof, d_vals, d_x, d_y, st);
+        return spmm_t_typed<double, double>(N, D, L.colptr, vin, L.rowof, d_vals, d_x, d_y, inv, st);
     if (vals_dtype == NIF_F64)
-        return spmm_t_typed<double, float>(N, D, L.colptr, vin, L.rowof, d_vals, d_x, d_y, st);
+        return spmm_t_typed<double, float>(N, D, L.colptr, vin, L.rowof, d_vals, d_x, d_y, inv, st);
     if (x_dtype == NIF_F64)
-        return spmm_t_typed<float, double>(N, D, L.colptr, vin, L.rowof, d_vals, d_x, d_y, st);
-    return spmm_t_typed<float, float>(N, D, L.colptr, vin, L.rowof, d_vals, d_x, d_y, st);
+        return spmm_t_typed<float, double>(N, D, L.colptr, vin, L.rowof, d_vals, d_x, d_y, inv, st);
+    return spmm_t_typed<float, float>(N, D, L.colptr, vin, L.rowof, d_vals, d_x, d_y, inv, st);
+}
+}  // namespace
+
+NIF_EXPORT int nif_spmm_t(int64_t M, int64_t N, int64_t nnz, const int32_t *d_rowptr,
+                          const int32_t *d_cols, const void *d_vals, int vals_dtype, const void *d_x,
+                          int x_dtype, int D, void *d_y, int y_dtype, void *d_ws, size_t ws_bytes,
+                          void *stream) {
+    return spmm_t_impl(M, N, nnz, d_rowptr, d_cols, d_vals, vals_dtype, d_x, x_dtype, D, d_y, y_dtype,
+                       nullptr, d_ws, ws_bytes, stream);
+}
+
+NIF_EXPORT int nif_spmm_t_ordered(int64_t M, int64_t N, int64_t nnz, const int32_t *d_rowptr,
+                                  const int32_t *d_cols, const void *d_vals, int vals_dtype,
+                                  const void *d_x, int x_dtype, int D, void *d_y, int y_dtype,
+                                  const int32_t *d_key_rank, void *d_ws, size_t ws_bytes,
+                                  void *stream) {
+    if (N > 0 && !d_key_rank) return NIF_ERR_ARG;
+    return spmm_t_impl(M, N, nnz, d_rowptr, d_cols, d_vals, vals_dtype, d_x, x_dtype, D, d_y, y_dtype,
+                       d_key_rank, d_ws, ws_bytes, stream);
 }
 
 namespace {
@@ -2574,6 +2754,87 @@ void grad_typed(const nif_dmesh *m, const void *q, int64_t M, const Centroid &ce
     run_rows(m, static_cast<const QT *>(q), M, cen, L, sink, st);
 }
 }  // namespace
+
+namespace {
+// the gradient rows from the forward's records: the volume kernel per chunk
+// of records, the forward's wide rows through the fused kernel, and the
+// forward's large-row queue through the large kernel (the same rows and
+// capacities as the forward, so the passes queue nothing new)
+template <class QT, class VT>
+void grad_records_typed(const nif_dmesh *m, const void *q, int64_t M, const Centroid &cen,
+                        const void *v, int D, const void *gout, const int32_t *rowptr,
+                        const double *w, const double *tot, void *gq, const QueryLayout &L,
+                        const RecordLayout &R, cudaStream_t st) {
+    using GT = typename std::conditional<(sizeof(QT) == 8 || sizeof(VT) == 8), double, float>::type;
+    using Sink = GradSink<QT, VT, GT>;
+    Sink sink{static_cast<const VT *>(v), static_cast<const GT *>(gout), rowptr, w, tot,
+              static_cast<QT *>(gq), D};
+    const QT *Q = static_cast<const QT *>(q);
+    constexpr int GPB = FAST_BLOCK / FAST_G;
+    const Launch lc{m->tune.tile, m->num_sms};
+    const OneMesh rows{m->view, cen};
+    cudaMemsetAsync(R.sum, 0, sizeof(DevSummary), st);
+    for (int64_t c0 = 0; c0 < M; c0 += REC_CHUNK) {
+        const int64_t n = min((int64_t)REC_CHUNK, M - c0);
+        launch_rows(k_rows_volume<QT, OneMesh, Sink, Sink::MIN_BLOCKS>, lc, n, GPB * sizeof(VolWS),
+                    R.counter, st, rows, Q, L.order + c0, n, (const RowHead *)(R.heads + c0),
+                    (const RowEntry *)(R.ents + c0 * REC_CAV), sink, LargeQueue{R.requeue}, R.sum);
+    }
+    const RowSet W{L.wide, &L.sum->wide_count, R.requeue, R.sum, R.counter, nullptr};
+    launch_fast_loc<QT, Sink, PM_PLAIN>(m, Q, M, cen, W, sink, st);
+    cudaMemcpyAsync(R.large_sum, L.sum, sizeof(DevSummary), cudaMemcpyDeviceToDevice, st);
+    k_rows_large<QT, Sink><<<LARGE_GROUPS, 32, 0, st>>>(m->view, Q, cen, LargeQueue{L.large_list},
+                                                        sink, L.large_ws, L.exact, R.large_sum);
+}
+}  // namespace
+
+NIF_EXPORT int nif_query_grad_records(const nif_dmesh *m, const void *d_queries, int query_dtype,
+                                      int64_t M, const double centroid[3], const int32_t *d_rowptr,
+                                      const double *d_weights, const double *d_row_totals,
+                                      const void *d_values, int values_dtype, int D,
+                                      const void *d_gout, int gout_dtype, void *d_gq,
+                                      const void *d_ws, size_t ws_bytes, void *d_records,
+                                      size_t records_bytes, void *stream, nif_summary *summary) {
+    int rc = check_query_args(m, d_queries, query_dtype, M, centroid, d_ws);
+    if (rc != NIF_OK) return rc;
+    if (m->view.pmode != PRED_FAST || !d_records) return NIF_ERR_ARG;
+    if (reinterpret_cast<uintptr_t>(d_records) % 256 != 0) return NIF_ERR_ARG;
+    if ((values_dtype != NIF_F64 && values_dtype != NIF_F32) || D < 1) return NIF_ERR_ARG;
+    if (gout_dtype != expect_promoted(query_dtype, values_dtype)) return NIF_ERR_ARG;
+    if (M > 0 && (!d_values || !d_gout || !d_gq || !d_rowptr || !d_row_totals)) return NIF_ERR_ARG;
+    size_t need = 0, rneed = 0;
+    nif_query_workspace_bytes(m, M, NIF_MODE_WEIGHTS, &need);
+    if (ws_bytes < need) return NIF_ERR_WORKSPACE;
+    nif_records_bytes(M, &rneed);
+    if (records_bytes < rneed) return NIF_ERR_WORKSPACE;
+    cudaStream_t st = S(stream);
+    Carve c{reinterpret_cast<unsigned char *>(const_cast<void *>(d_ws)), 0, ws_bytes, true};
+    const QueryLayout L = carve_query(c, M, NIF_MODE_WEIGHTS);
+    Carve cr{static_cast<unsigned char *>(d_records), 0, records_bytes, true};
+    const RecordLayout R = carve_records(cr, M);
+    Centroid cen{{centroid[0], centroid[1], centroid[2]}};
+    if (M > 0) {
+        if (query_dtype == NIF_F64 && values_dtype == NIF_F64)
+            grad_records_typed<double, double>(m, d_queries, M, cen, d_values, D, d_gout, d_rowptr,
+                                               d_weights, d_row_totals, d_gq, L, R, st);
+        else if (query_dtype == NIF_F64)
+            grad_records_typed<double, float>(m, d_queries, M, cen, d_values, D, d_gout, d_rowptr,
+                                              d_weights, d_row_totals, d_gq, L, R, st);
+        else if (values_dtype == NIF_F32)
+            grad_records_typed<float, float>(m, d_queries, M, cen, d_values, D, d_gout, d_rowptr,
+                                             d_weights, d_row_totals, d_gq, L, R, st);
+        else
+            grad_records_typed<float, double>(m, d_queries, M, cen, d_values, D, d_gout, d_rowptr,
+                                              d_weights, d_row_totals, d_gq, L, R, st);
+    }
+    if (summary) {
+        // the gradient pass's own counters (its rows are the forward's)
+        QueryLayout G = L;
+        G.sum = R.sum;
+        return read_summary(G, st, summary, nullptr);
+    }
+    return cuda_rc(cudaGetLastError());
+}
 
 NIF_EXPORT int nif_query_grad(const nif_dmesh *m, const void *d_queries, int query_dtype, int64_t M,
                               const double centroid[3], const int32_t *d_rowptr,
@@ -2885,14 +3146,23 @@ void batch_typed(const nif_dbatch *b, const void *q, int64_t M, const int64_t *q
     launch_scan<int>(L.bcount, nbk, L.bsum, L.btotal, L.bcount, st);
     k_scatter<<<blocks_for(M, 256), 256, 0, st>>>(L.bucket, M, L.bcount, L.order);
     Sink sink{static_cast<const VT *>(v), koff, qoff, b->P, static_cast<CT *>(out), D};
+    // the split row kernels, rows mapped to their problems' meshes (filtered
+    // predicates where any problem's mesh asks for them: the kernels test
+    // each mesh's own mode); then the rows whose cavity exceeds a record
+    // through the fused kernel
+    const Launch lc{b->tune.tile, b->num_sms};
+    const ManyMeshes rows{b->d_views, qoff, b->P, cens};
+    const RowSet R{L.order, nullptr, L.large_list, L.sum, L.counter, L.located};
     if (b->filtered) {
-        launch_batch_rows<QT, Sink, PM_FILTER>(b, Q, M, qoff, cens, sink, L, st, L.order);
+        if (b->tune.blocks_per_sm == OCC_LO)
+            launch_split<QT, ManyMeshes, Sink, OCC_LO, PM_FILTER>(lc, rows, Q, M, R, L.heads, L.ents,
+                                                                  L.wide, sink, st);
+        else
+            launch_split<QT, ManyMeshes, Sink, OCC_HI, PM_FILTER>(lc, rows, Q, M, R, L.heads, L.ents,
+                                                                  L.wide, sink, st);
+        launch_batch_rows<QT, Sink, PM_FILTER>(b, Q, M, qoff, cens, sink, L, st, L.wide,
+                                               &L.sum->wide_count);
     } else {
-        // the split row kernels, rows mapped to their problems' meshes; then
-        // the rows whose cavity exceeds a record through the fused kernel
-        const Launch lc{b->tune.tile, b->num_sms};
-        const ManyMeshes rows{b->d_views, qoff, b->P, cens};
-        const RowSet R{L.order, nullptr, L.large_list, L.sum, L.counter, L.located};
         if (b->tune.blocks_per_sm == OCC_LO)
             launch_split<QT, ManyMeshes, Sink, OCC_LO>(lc, rows, Q, M, R, L.heads, L.ents, L.wide, sink, st);
         else
@@ -3028,7 +3298,7 @@ NIF_EXPORT int nif_batch_summary(const nif_dbatch *b, int64_t total_queries, con
     summary->rows_outside = (int64_t)d.rows_outside;
     summary->walk_steps = (int64_t)d.walk_steps;
     summary->first_status = d.first_status;
-    summary->reserved = 0;
+    summary->rows_wide = d.wide_count;
     summary->orient_uncertain = (int64_t)d.orient_unc;
     summary->orient_flipped = (int64_t)d.orient_flip;
     summary->insphere_uncertain = (int64_t)d.insphere_unc;

@@ -34,8 +34,8 @@
 #include <math.h>
 
 #ifdef __CUDACC__
-#define NIF_XI __host__ __device__ __forceinline__
-#define NIF_XF __host__ __device__ __noinline__
+#define NIF_XI static __host__ __device__ __forceinline__
+#define NIF_XF static __host__ __device__ __noinline__
 #else
 #define NIF_XI static inline
 #define NIF_XF static __attribute__((unused))

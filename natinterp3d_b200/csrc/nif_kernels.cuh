@@ -1280,12 +1280,14 @@ __device__ RowInfo sibson_row(const MeshView &M, const dv3 q, W &ws, const Grp<G
 // REC_WIDE where the cavity fits the shared-memory capacities but not the
 // record (the caller queues the row for the fused row kernel), or REC_LARGE
 // where it exceeds the shared-memory capacities (the large kernel's).
+// With PM_FILTER a test the error bound cannot certify also gives REC_LARGE
+// (the large kernel resolves it exactly).
 constexpr int REC_DONE = 0, REC_WIDE = 1, REC_LARGE = 2;
-template <int G, class W>
+template <int G, class W, int PM = PM_PLAIN>
 __device__ int cavity_record(const MeshView &M, const dv3 q, W &ws, const Grp<G> &g, int start,
                              RowHead &head, RowEntry *__restrict__ ent) {
     RowInfo r{ST_OK, 0, 0, false, false, 0.0, 0, 0, 0, 0, 0};
-    const int ncav = flood_replay<G, W, PM_PLAIN>(M, q, ws, g, start, r, false, nullptr);
+    const int ncav = flood_replay<G, W, PM>(M, q, ws, g, start, r, false, nullptr);
     if (r.status != ST_OK) return REC_LARGE;
     if (ncav > REC_CAV) return REC_WIDE;
     head.ncav = ncav;

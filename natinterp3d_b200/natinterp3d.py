@@ -20,11 +20,22 @@ natinterp3d's behaviour and the default; 'audit' gives identical results and
 counts the predicate evaluations that the static error bound cannot certify
 (``predicate_stats``); 'exact' decides them exactly.
 
+``constructor`` (an extension) selects who builds the tetrahedralization:
+'host' (the default) is natinterp3d's own constructor; 'gpu' builds the same
+Delaunay tetrahedralization of keys + super-simplex on the GPU with exact
+predicates (``construction`` reports its counters and checks).  For keys in
+general position the two give the same set of tets, stored in another order,
+so weights agree to rounding and the column order of a row may differ.  Key
+sets that are degenerate for exact arithmetic (which natinterp3d perturbs
+randomly) fall back to the host constructor with a warning.
+
 Device-resident variants (``get_weights_device``, ``interpolate_device``)
 take and return torch tensors on the mesh's GPU.
 """
 import os
 from typing import Optional
+
+import warnings
 
 import numpy as np
 import scipy.sparse
@@ -32,7 +43,7 @@ import torch
 
 from . import _native as N
 from ._native import HostMesh
-from .device import DeviceMesh
+from .device import DeviceMesh, GPUConstructionError, gpu_delaunay
 
 _FLOATS = (np.dtype(np.float32), np.dtype(np.float64))
 PIPELINE_CHUNK = 1 << 21  # queries per chunk of the pipelined host interpolation
@@ -138,6 +149,9 @@ class Interpolator:
         keep_host_mesh: keep natinterp3d's host mesh object alive (only needed
             to run natinterp3d's CPU query on the same mesh for comparison).
         predicates: 'fast' (natinterp3d's non-robust signs), 'audit' or 'exact'.
+        constructor: 'host' (natinterp3d's constructor) or 'gpu' (the same
+            Delaunay tetrahedralization built on the GPU; degenerate key sets
+            fall back to 'host').
     """
 
     def __init__(
@@ -148,26 +162,55 @@ class Interpolator:
         device=None,
         keep_host_mesh: bool = False,
         predicates: str = 'fast',
+        constructor: str = 'host',
     ):
         data_points = np.ascontiguousarray(data_points, np.float64)
         if data_points.ndim != 2 or data_points.shape[1] != 3:
             raise ValueError('Data points must have shape (num_data_points, 3)')
+        if constructor not in ('host', 'gpu'):
+            raise ValueError("constructor must be 'host' or 'gpu'")
         # natinterp3d.py:88-90: centre on the key centroid before triangulating
         self._centroid = data_points.mean(axis=0)
         centered = data_points - self._centroid
         self.n_keys = int(data_points.shape[0])
         self.parallel = parallel
         self.num_threads = num_threads
-        host = HostMesh(centered)
-        self.degeneracies = host.degeneracies()
-        self.mesh_arrays = host.export()
-        self.host_mesh = host if keep_host_mesh else None
-        if not keep_host_mesh:
-            host.close()
         self._device_arg = device
         self._dmesh = None
+        self._mesh_arrays = None
+        self._mesh_dev = None
+        self.host_mesh = None
+        self.construction = {'constructor': 'host'}
+        if constructor == 'gpu':
+            try:
+                self._mesh_dev, info = gpu_delaunay(centered, device)
+                self.construction = dict(info, constructor='gpu')
+                self.degeneracies = {'coplanar': 0, 'cospherical': 0}
+            except GPUConstructionError as e:
+                warnings.warn('%s; using natinterp3d\'s host constructor' % e, RuntimeWarning)
+                self.construction = dict(e.info, constructor='host', gpu_declined=str(e))
+        if self._mesh_dev is None:
+            host = HostMesh(centered)
+            self.degeneracies = host.degeneracies()
+            self._mesh_arrays = host.export()
+            self.host_mesh = host if keep_host_mesh else None
+            if not keep_host_mesh:
+                host.close()
         self._predicates = 'fast'
         self.set_predicates(predicates)
+
+    @property
+    def mesh_arrays(self):
+        """(vxyz, tet_v, tet_n): the packed mesh as numpy arrays (copied from
+        the device on first use for a GPU-built mesh)."""
+        if self._mesh_arrays is None and getattr(self, '_mesh_dev', None) is not None:
+            self._mesh_arrays = tuple(t.cpu().numpy() for t in self._mesh_dev)
+        return self._mesh_arrays
+
+    @mesh_arrays.setter
+    def mesh_arrays(self, arrays):
+        self._mesh_arrays = arrays
+        self._mesh_dev = None
 
     @classmethod
     def from_mesh(cls, centroid, vxyz, tet_v, tet_n, device=None, predicates='fast'):
@@ -181,6 +224,7 @@ class Interpolator:
         self.parallel, self.num_threads = True, None
         self.degeneracies = None
         self.host_mesh = None
+        self.construction = {'constructor': 'saved mesh'}
         self._device_arg = device
         self._dmesh = None
         self._predicates = 'fast'
@@ -213,7 +257,8 @@ class Interpolator:
         return {'format': 1, 'centroid': self._centroid, 'vxyz': vxyz, 'tet_v': tet_v,
                 'tet_n': tet_n, 'parallel': self.parallel, 'num_threads': self.num_threads,
                 'degeneracies': self.degeneracies, 'predicates': self._predicates,
-                'tuning': getattr(self, '_tuning', None), 'device': dev}
+                'tuning': getattr(self, '_tuning', None), 'device': dev,
+                'construction': getattr(self, 'construction', None)}
 
     def __setstate__(self, state):
         if state.get('format') != 1:
@@ -233,6 +278,7 @@ class Interpolator:
         self._dmesh = None
         self._predicates = state['predicates']
         self._tuning = state['tuning']
+        self.construction = state.get('construction') or {'constructor': 'host'}
 
     @property
     def centroid(self):
@@ -241,7 +287,9 @@ class Interpolator:
     @property
     def device_mesh(self) -> DeviceMesh:
         if self._dmesh is None:
-            self._dmesh = DeviceMesh(*self.mesh_arrays, device=self._device_arg)
+            src = getattr(self, '_mesh_dev', None)
+            self._dmesh = DeviceMesh(*(src if src is not None else self.mesh_arrays),
+                                     device=self._device_arg)
             self._dmesh.set_predicates(self._predicates)
             if getattr(self, '_tuning', None) is not None:
                 self._dmesh.set_tuning(self._tuning)

@@ -105,3 +105,40 @@ def test_float32_inputs_and_module(cuda_device):
     out.sum().backward()
     assert q.grad.dtype == torch.float32 and torch.isfinite(q.grad).all()
     assert v.grad.shape == (2000,) and v.grad.dtype == torch.float32
+
+
+def test_ordered_transpose_product_is_bit_identical(cuda_device):
+    # the transpose product with the columns visited in a caller-given order
+    # (the mesh's spatial key order, or any permutation) equals the plain one
+    # and scipy's W.T @ x bit for bit
+    import ctypes
+    from natinterp3d_b200 import _native as N
+    from natinterp3d_b200.device import _vp, _stream_ptr
+    rng = np.random.default_rng(17)
+    M, Ncol, D = 5000, 3000, 5
+    W = scipy.sparse.random(M, Ncol, density=0.004, format='csr', random_state=3, dtype=np.float64)
+    x = rng.standard_normal((M, D))
+    dev = cuda_device
+    rowptr = torch.from_numpy(W.indptr.astype(np.int32)).to(dev)
+    cols = torch.from_numpy(W.indices.astype(np.int32)).to(dev)
+    vals = torch.from_numpy(W.data).to(dev)
+    xd = torch.from_numpy(x).to(dev)
+    rank = torch.from_numpy(rng.permutation(Ncol).astype(np.int32)).to(dev)
+    lib = N.cuda_lib()
+    nb = ctypes.c_size_t()
+    N.check(lib.nif_spmm_t_workspace_bytes(M, Ncol, W.nnz, ctypes.byref(nb)), 'ws')
+    ws = torch.empty(int(nb.value), dtype=torch.uint8, device=dev)
+    outs = []
+    for ordered in (False, True):
+        y = torch.empty((Ncol, D), dtype=torch.float64, device=dev)
+        args = [M, Ncol, W.nnz, _vp(rowptr), _vp(cols), _vp(vals), N.NIF_F64, _vp(xd), N.NIF_F64, D,
+                _vp(y), N.NIF_F64]
+        if ordered:
+            rc = lib.nif_spmm_t_ordered(*args, _vp(rank), _vp(ws), ws.numel(), _stream_ptr(dev))
+        else:
+            rc = lib.nif_spmm_t(*args, _vp(ws), ws.numel(), _stream_ptr(dev))
+        N.check(rc, 'spmm_t')
+        outs.append(y.cpu().numpy())
+    assert np.array_equal(outs[0].view(np.uint8), outs[1].view(np.uint8))
+    ref = W.T.tocsr() @ x
+    assert np.abs(outs[1] - ref).max() < 1e-12
