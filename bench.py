@@ -726,7 +726,7 @@ def main():
     # read once here: the loop itself never waits on the host)
     ph = (ctypes.c_double * 4)()
     have_phases = lib.nif_profile_read(ph) == 0
-    kms, kn = (ctypes.c_double * 4)(), (ctypes.c_double * 4)()
+    kms, kn = (ctypes.c_double * 5)(), (ctypes.c_double * 5)()
     lib.nif_profile_kernels(kms, kn)
     lib.nif_profile_enable(0)
     ms = e0.elapsed_time(e1) / args.steps
@@ -764,7 +764,7 @@ def main():
         vol_ms, vol_launches = kms[2], kn[2]
         achieved = (fpq['volume'] * vol_rows / (vol_ms * 1e-3) / 1e12) if vol_ms > 0 else None
         path_achieved = fpq['total'] * M / (rows_ms * 1e-3) / 1e12 if rows_ms > 0 else None
-        names = ['k_locate', 'k_rows_cavity', 'k_rows_volume', 'k_rows_fast']
+        names = ['k_locate', 'k_rows_cavity', 'k_rows_volume', 'k_rows_fast', 'k_rows_order']
         kernels = {n: {'ms_per_step': kms[i], 'launches_per_step': kn[i],
                        'share_of_rows_phase': kms[i] / rows_ms if rows_ms > 0 else None}
                    for i, n in enumerate(names)}
@@ -805,7 +805,7 @@ def main():
                             if vol_launches else None),
                 'traffic_note': 'per launch; ncu capture of %s' % TRAFFIC_SOURCE,
                 'row_path': {
-                    'kernels': 'k_locate + k_rows_cavity + k_rows_volume (+ k_rows_fast)',
+                    'kernels': 'k_locate + k_rows_cavity + k_rows_order + k_rows_volume (+ k_rows_fast)',
                     'achieved': path_achieved, 'flops_per_query': fpq['total'],
                     'frac': (path_achieved / separate.value) if path_achieved and separate.value
                     else None,

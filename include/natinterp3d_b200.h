@@ -390,11 +390,11 @@ int nif_batch_summary(const nif_dbatch *b, int64_t total_queries, const void *d_
  * enable or read (at most the last 64).  (natinterp3d has no counterpart.)
  * nif_profile_kernels then returns, for the same calls, the device time in
  * milliseconds and the launches per call of each row kernel: {k_locate,
- * k_rows_cavity, k_rows_volume, k_rows_fast} (events bracket each launch,
- * at most 48 a call). */
+ * k_rows_cavity, k_rows_volume, k_rows_fast, k_rows_order} (events bracket
+ * each launch, at most 48 a call). */
 int nif_profile_enable(int on);
 int nif_profile_read(double ms[4]);
-int nif_profile_kernels(double ms[4], double launches[4]);
+int nif_profile_kernels(double ms[5], double launches[5]);
 
 /* Measured FP64 throughput of the current device in TFLOP/s (2 flops per
  * multiply-add pair), with fused multiply-add and with separately rounded

@@ -1188,6 +1188,121 @@ __global__ void __launch_bounds__(FAST_BLOCK, OCC)
     }
 }
 
+// The split rows' visiting order: each record gets natinterp3d's LIFO
+// visiting order (natural_insertionfree.c:486-551, replayed on the cavity;
+// its non-cavity tets are leaves and do not change the order) and the fcc[]
+// indices of its faces as natinterp3d's face cache returns them (a face
+// shared with a cavity tet visited earlier reads that tet's copy through the
+// mirror slot, natural_insertionfree.c:233-253).  One warp takes 32
+// consecutive rows: the lanes load the rows' neighbour tables into shared
+// memory entry by entry, each lane replays one row there, and the lanes
+// write the positions and face choices back entry by entry.  Rows without a
+// cavity record are left alone.
+constexpr int ORD_WARPS = 2;
+constexpr int ORD_PAD = REC_CAV + 1;  // row stride of the shared tables (banks)
+struct OrderWS {
+    int nbr[32][ORD_PAD];
+    int tet[32][ORD_PAD];
+    int8_t stack[32][4 * REC_CAV + 1];
+    int8_t pos[32][REC_CAV];
+    uint8_t mir[32][REC_CAV];
+    int start[33];
+};
+
+__global__ void __launch_bounds__(32 * ORD_WARPS) k_rows_order(int64_t nrows, const RowHead *__restrict__ heads,
+                                                               RowEntry *__restrict__ ents) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    OrderWS &w = reinterpret_cast<OrderWS *>(smem)[threadIdx.x >> 5];
+    const int lane = threadIdx.x & 31;
+    const unsigned full = 0xffffffffu;
+    const int64_t ngroups = (nrows + 31) / 32;
+    for (int64_t gi = (int64_t)blockIdx.x * ORD_WARPS + (threadIdx.x >> 5); gi < ngroups;
+         gi += (int64_t)gridDim.x * ORD_WARPS) {
+        const int64_t s0 = gi * 32;
+        const int64_t s = s0 + lane;
+        int nc = 0;
+        if (s < nrows) {
+            const RowHead h = heads[s];
+            if (h.state == RS_OK && h.ncav > 0 && h.ncav <= REC_CAV) nc = h.ncav;
+        }
+        // entry offsets of the 32 rows in one flattened index space
+        int incl = nc;
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            const int v = __shfl_up_sync(full, incl, off);
+            if (lane >= off) incl += v;
+        }
+        w.start[lane] = incl - nc;
+        if (lane == 31) w.start[32] = incl;
+        __syncwarp();
+        const int total = w.start[32];
+        // row of flattened entry k: the last row whose start is <= k
+        auto row_of = [&](int k) {
+            int lo = 0, hi = 32;  // start[lo] <= k < start[hi]
+            while (hi - lo > 1) {
+                const int mid = (lo + hi) >> 1;
+                if (w.start[mid] <= k) lo = mid; else hi = mid;
+            }
+            // skip empty rows that share the start
+            while (w.start[lo + 1] <= k) lo++;
+            return lo;
+        };
+        for (int k = lane; k < total; k += 32) {
+            const int j = row_of(k), e = k - w.start[j];
+            const RowEntry x = ents[(s0 + j) * REC_CAV + e];
+            w.nbr[j][e] = x.nbr;
+            w.tet[j][e] = x.tet;
+            w.mir[j][e] = (uint8_t)(x.bmask >> 8);
+        }
+        __syncwarp();
+        if (nc > 0) {
+            int8_t *stack = w.stack[lane];
+            int8_t *pos = w.pos[lane];
+            const int *nb = w.nbr[lane];
+            for (int c = 0; c < nc; c++) pos[c] = 0;
+            uint64_t vis = 0;
+            int sp = 0, nord = 0;
+            stack[sp++] = 0;  // the flood put the located tet first
+            while (sp > 0) {
+                const int c = stack[--sp];
+                if ((vis >> c) & 1ull) continue;
+                vis |= 1ull << c;
+                pos[c] = (int8_t)nord++;
+                const unsigned wd = (unsigned)nb[c];
+#pragma unroll
+                for (int f = 0; f < 4; f++) {
+                    const int n = (int8_t)((wd >> (8 * f)) & 0xffu);
+                    if (n >= 0 && !((vis >> n) & 1ull)) stack[sp++] = (int8_t)n;
+                }
+            }
+        }
+        __syncwarp();
+        for (int k = lane; k < total; k += 32) {
+            const int j = row_of(k), e = k - w.start[j];
+            const unsigned wd = (unsigned)w.nbr[j][e];
+            const int tt = w.tet[j][e];
+            const unsigned mir = w.mir[j][e];
+            const int pe = w.pos[j][e];
+            int fp[4];
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+                const int jf = 3 - i;
+                const int n = (int8_t)((wd >> (8 * jf)) & 0xffu);
+                if (n >= 0 && w.pos[j][n] < pe) {
+                    const int jm = (mir >> (2 * jf)) & 3;
+                    fp[i] = 4 * w.tet[j][n] + (3 - jm);
+                } else {
+                    fp[i] = 4 * tt + i;
+                }
+            }
+            RowEntry *E = ents + (s0 + j) * REC_CAV + e;
+            E->fp = make_int4(fp[0], fp[1], fp[2], fp[3]);
+            E->pos = pe;
+        }
+        __syncwarp();
+    }
+}
+
 template <class QT, class Rows, class Sink, int OCC>
 __global__ void __launch_bounds__(FAST_BLOCK, OCC)
     k_rows_volume(const __grid_constant__ Rows rows, const QT *__restrict__ Q,
@@ -1618,8 +1733,8 @@ int resident_blocks(Kern k, int threads, size_t smem) {
 constexpr int PROF_EVENTS = 5;  // start | bucketing | fast rows | large rows | finish
 constexpr int PROF_RING = 64;
 constexpr int PROF_SPANS = 48;  // kernel spans recorded per call (further launches are not)
-constexpr int PROF_KINDS = 4;   // k_locate | k_rows_cavity | k_rows_volume | k_rows_fast
-enum { SPAN_LOCATE = 0, SPAN_CAVITY = 1, SPAN_VOLUME = 2, SPAN_FUSED = 3 };
+constexpr int PROF_KINDS = 5;   // k_locate | k_rows_cavity | k_rows_volume | k_rows_fast | k_rows_order
+enum { SPAN_LOCATE = 0, SPAN_CAVITY = 1, SPAN_VOLUME = 2, SPAN_FUSED = 3, SPAN_ORDER = 4 };
 struct Profiler {
     bool on = false;
     bool created = false;
@@ -1802,6 +1917,15 @@ void launch_split(const Launch &lc, const Rows &rows, const QT *Q, int64_t M, co
                     rows, Q, R.order + c0, n, (const int *)located, h, e, wide, LargeQueue{R.large},
                     R.sum);
         prof_span(SPAN_CAVITY, true, st);
+        prof_span(SPAN_ORDER, false, st);
+        {
+            const int64_t groups = (n + 31) / 32;
+            int64_t ob = (groups + ORD_WARPS - 1) / ORD_WARPS;
+            if (ob > (int64_t)lc.num_sms * 32) ob = (int64_t)lc.num_sms * 32;
+            k_rows_order<<<(unsigned)ob, 32 * ORD_WARPS, ORD_WARPS * sizeof(OrderWS), st>>>(
+                n, (const RowHead *)h, e);
+        }
+        prof_span(SPAN_ORDER, true, st);
         prof_span(SPAN_VOLUME, false, st);
         launch_rows(k_rows_volume<QT, Rows, Sink, VOCC>, lc, n, GPB * sizeof(VolWS), R.counter, st,
                     rows, Q, R.order + c0, n, (const RowHead *)h, (const RowEntry *)e, sink,
@@ -2417,7 +2541,7 @@ NIF_EXPORT int nif_profile_read(double ms[4]) {
     return NIF_OK;
 }
 
-NIF_EXPORT int nif_profile_kernels(double ms[4], double launches[4]) {
+NIF_EXPORT int nif_profile_kernels(double ms[5], double launches[5]) {
     if (!ms || !launches) return NIF_ERR_ARG;
     for (int k = 0; k < PROF_KINDS; k++) {
         ms[k] = g_prof.kms[k];

@@ -92,7 +92,7 @@ struct State {
 struct Cavity {
     long long off;
     int ncav, nbf;
-    int status;  // 0 ok, 1 skipped this round, 2 failed
+    int status;  // 0 ok, 1 skipped this round, 2 failed, 3 outranked nearby (no flood)
     int pad;
 };
 
@@ -374,6 +374,33 @@ __global__ void __launch_bounds__(THREADS) k_cavity(Dev D, int round) {
         const unsigned long long key = key_of(round, p);
         const dv3 P = P3(D.pts[p]);
         const int t0 = D.ptet[p];
+        // A nominee within two tet steps of a nominee with a lower priority
+        // skips the flood: their claims would meet in a tet adjacent to both
+        // start tets, so it could only win if that nominee did not claim.
+        // Every nominee that would win without this test passes it (all the
+        // nominees it conflicts with have higher priorities), and the
+        // nominees it removes claim nothing, so no winner is lost.
+        bool lower = false;
+        if (lane < 16) {
+            const int n1 = comp4(D.tn[t0], lane >> 2);
+            if (n1 >= 0) {
+                lower = D.nom[n1] < key;
+                const int n2 = comp4(D.tn[n1], lane & 3);
+                if (n2 >= 0 && D.nom[n2] < key) lower = true;
+            }
+        }
+        if (__any_sync(FULL, lower)) {
+            if (lane == 0) {
+                Cavity cv;
+                cv.off = 0;
+                cv.ncav = cv.nbf = 0;
+                cv.status = 3;
+                cv.pad = 0;
+                D.cav[i] = cv;
+            }
+            __syncwarp();
+            continue;
+        }
         for (int k = lane; k < HS; k += 32) w.hkey[k] = -1;
         __syncwarp();
         if (lane == 0) {

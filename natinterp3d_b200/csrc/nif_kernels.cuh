@@ -531,12 +531,16 @@ struct VolWorkspace {
     uint16_t bface[BF_];
     int16_t vh_slot[VH_];
     uint8_t bmask[CAV_];  // boundary faces of each cavity tet, one bit per face
+    uint8_t eidx[CAV_];   // record entry of the o-th visited cavity tet
 };
 
-// One row between k_rows_cavity and k_rows_volume: a header and, per cavity
-// tet in natinterp3d's visiting order, the tet, the fcc[] indices of its
-// faces' circumcentres as natinterp3d's face cache returns them, and which
-// of its faces bound the cavity.
+// One row between k_rows_cavity, k_rows_order and k_rows_volume: a header
+// and, per cavity tet in the flood's order, the tet, which of its faces bound
+// the cavity (bits 0-3) and the mirror slots of its faces (bits 8-15, the
+// mesh's tinfo bits 8-15), the cavity indices of its four neighbours (four
+// signed bytes, -1 outside the cavity); k_rows_order adds the tet's position
+// in natinterp3d's visiting order and the fcc[] indices of its faces'
+// circumcentres as natinterp3d's face cache returns them.
 constexpr int REC_CAV = 48;  // cavity tets a record holds (larger cavities take the large kernel)
 constexpr int RS_OK = 0, RS_OUTSIDE = 1, RS_WALK = 2, RS_QUEUED = 3;
 struct __align__(16) RowHead {
@@ -548,8 +552,9 @@ struct __align__(16) RowHead {
 struct __align__(32) RowEntry {
     int4 fp;
     int tet;
-    unsigned bmask;
-    int pad[2];
+    unsigned bmask;  // boundary faces | mirror slots << 8
+    int nbr;         // cavity indices of neighbours 0..3, one signed byte each
+    int pos;         // position in natinterp3d's visiting order
 };
 
 __device__ __forceinline__ unsigned mix_hash(int key) {
@@ -798,8 +803,9 @@ __device__ int locate(const MeshView &M, const dv3 q, const Grp<G> &g, int *scra
 // the cavity index of the o-th visited, ws.pos its inverse and ws.cav_nbr
 // [4c + f] the cavity index of neighbour f of cavity tet c (-1 outside).  On
 // overflow / an uncertain test (PM_FILTER) r.status is set; an empty cavity
-// (0) leaves the order unset.
-template <int G, class W, int PM>
+// (0) leaves the order unset.  REPLAY = false stops after the flood and the
+// neighbour table (the split row path replays the order in k_rows_order).
+template <int G, class W, int PM, bool REPLAY = true>
 __device__ int flood_replay(const MeshView &M, const dv3 q, W &ws, const Grp<G> &g, const int start,
                             RowInfo &r, const bool on_face, double *xs) {
     using cav_t = typename W::cav_t;
@@ -915,64 +921,68 @@ __device__ int flood_replay(const MeshView &M, const dv3 q, W &ws, const Grp<G> 
     // cavity-local neighbour table: cav_nbr[4c+f] = cavity index of s[f] or -1
     // (every neighbour slot recorded by the flood has been tested by now)
     for (int k = g.lane; k < 4 * ncav; k += G) ws.cav_nbr[k] = ws.u.a.hval[nsl[k]];
-    for (int c = g.lane; c < ncav; c += G) ws.pos[c] = (cav_t)-1;
-    g.sync();
+    if constexpr (!REPLAY) {
+        g.sync();
+    } else {
+        for (int c = g.lane; c < ncav; c += G) ws.pos[c] = (cav_t)-1;
+        g.sync();
 
-    // cavity index 0 is the located tet, the flood's start
-    int start_c = 0;
-    if constexpr (PM == PM_RESOLVE) {
-        if (on_face && M.pmode == PRED_EXACT) start_c = canonical_start(M, ws, g, xs, q, ncav);
-    }
+        // cavity index 0 is the located tet, the flood's start
+        int start_c = 0;
+        if constexpr (PM == PM_RESOLVE) {
+            if (on_face && M.pmode == PRED_EXACT) start_c = canonical_start(M, ws, g, xs, q, ncav);
+        }
 
-    // replay natinterp3d's LIFO flood on the cavity (its non-cavity tets are
-    // leaves and do not change the order in which cavity tets are reached)
-    if (g.lane == 0) {
-        cav_t *stack = ws.u.r.stack;
-        int sp = 0, nord = 0;
-        stack[sp++] = (cav_t)start_c;
-        if constexpr (W::CAV <= 128) {
-            // visited set in two 64-bit registers
-            uint64_t v0 = 0, v1 = 0;
-            while (sp > 0) {
-                const int c = stack[--sp];
-                const uint64_t bit = 1ull << (c & 63);
-                if ((c < 64 ? v0 : v1) & bit) continue;
-                if (c < 64) v0 |= bit; else v1 |= bit;
-                int n0, n1, n2, n3;
-                if constexpr (sizeof(cav_t) == 1) {
-                    // the four signed 8-bit entries of tet c in one 32-bit load
-                    const int w = *reinterpret_cast<const int *>(&ws.cav_nbr[4 * c]);
-                    n0 = (int8_t)(w & 0xff);
-                    n1 = (int8_t)((w >> 8) & 0xff);
-                    n2 = (int8_t)((w >> 16) & 0xff);
-                    n3 = (int8_t)((unsigned)w >> 24);
-                } else {
-                    n0 = ws.cav_nbr[4 * c], n1 = ws.cav_nbr[4 * c + 1];
-                    n2 = ws.cav_nbr[4 * c + 2], n3 = ws.cav_nbr[4 * c + 3];
+        // replay natinterp3d's LIFO flood on the cavity (its non-cavity tets are
+        // leaves and do not change the order in which cavity tets are reached)
+        if (g.lane == 0) {
+            cav_t *stack = ws.u.r.stack;
+            int sp = 0, nord = 0;
+            stack[sp++] = (cav_t)start_c;
+            if constexpr (W::CAV <= 128) {
+                // visited set in two 64-bit registers
+                uint64_t v0 = 0, v1 = 0;
+                while (sp > 0) {
+                    const int c = stack[--sp];
+                    const uint64_t bit = 1ull << (c & 63);
+                    if ((c < 64 ? v0 : v1) & bit) continue;
+                    if (c < 64) v0 |= bit; else v1 |= bit;
+                    int n0, n1, n2, n3;
+                    if constexpr (sizeof(cav_t) == 1) {
+                        // the four signed 8-bit entries of tet c in one 32-bit load
+                        const int w = *reinterpret_cast<const int *>(&ws.cav_nbr[4 * c]);
+                        n0 = (int8_t)(w & 0xff);
+                        n1 = (int8_t)((w >> 8) & 0xff);
+                        n2 = (int8_t)((w >> 16) & 0xff);
+                        n3 = (int8_t)((unsigned)w >> 24);
+                    } else {
+                        n0 = ws.cav_nbr[4 * c], n1 = ws.cav_nbr[4 * c + 1];
+                        n2 = ws.cav_nbr[4 * c + 2], n3 = ws.cav_nbr[4 * c + 3];
+                    }
+                    ws.pos[c] = (cav_t)nord;
+                    ws.order[nord++] = (cav_t)c;
+                    const int nb[4] = {n0, n1, n2, n3};
+    #pragma unroll
+                    for (int f = 0; f < 4; f++) {
+                        const int nc = nb[f];
+                        if (nc >= 0 && !(((nc < 64 ? v0 : v1) >> (nc & 63)) & 1ull)) stack[sp++] = (cav_t)nc;
+                    }
                 }
-                ws.pos[c] = (cav_t)nord;
-                ws.order[nord++] = (cav_t)c;
-                const int nb[4] = {n0, n1, n2, n3};
-#pragma unroll
-                for (int f = 0; f < 4; f++) {
-                    const int nc = nb[f];
-                    if (nc >= 0 && !(((nc < 64 ? v0 : v1) >> (nc & 63)) & 1ull)) stack[sp++] = (cav_t)nc;
-                }
-            }
-        } else {
-            while (sp > 0) {
-                const int c = stack[--sp];
-                if (ws.pos[c] >= 0) continue;
-                ws.pos[c] = (cav_t)nord;
-                ws.order[nord++] = (cav_t)c;
-                for (int f = 0; f < 4; f++) {
-                    const int nc = ws.cav_nbr[4 * c + f];
-                    if (nc >= 0 && ws.pos[nc] < 0) stack[sp++] = (cav_t)nc;
+            } else {
+                while (sp > 0) {
+                    const int c = stack[--sp];
+                    if (ws.pos[c] >= 0) continue;
+                    ws.pos[c] = (cav_t)nord;
+                    ws.order[nord++] = (cav_t)c;
+                    for (int f = 0; f < 4; f++) {
+                        const int nc = ws.cav_nbr[4 * c + f];
+                        if (nc >= 0 && ws.pos[nc] < 0) stack[sp++] = (cav_t)nc;
+                    }
                 }
             }
         }
+        g.sync();
     }
-    g.sync();
 
     return ncav;
 }
@@ -1286,24 +1296,30 @@ constexpr int REC_DONE = 0, REC_WIDE = 1, REC_LARGE = 2;
 template <int G, class W, int PM = PM_PLAIN>
 __device__ int cavity_record(const MeshView &M, const dv3 q, W &ws, const Grp<G> &g, int start,
                              RowHead &head, RowEntry *__restrict__ ent) {
+    static_assert(REC_CAV <= 127, "neighbour indices are signed bytes");
     RowInfo r{ST_OK, 0, 0, false, false, 0.0, 0, 0, 0, 0, 0};
-    const int ncav = flood_replay<G, W, PM>(M, q, ws, g, start, r, false, nullptr);
+    const int ncav = flood_replay<G, W, PM, false>(M, q, ws, g, start, r, false, nullptr);
     if (r.status != ST_OK) return REC_LARGE;
     if (ncav > REC_CAV) return REC_WIDE;
     head.ncav = ncav;
-    for (int o = g.lane; o < ncav; o += G) {
-        const int c = ws.order[o];
-        int fp[4];
-        face_cc_choice(M, ws, c, fp);
-        unsigned bm = 0;
+    for (int c = g.lane; c < ncav; c += G) {
+        const int tt = ws.cav_tet[c];
+        unsigned bm = (M.tinfo[tt] >> 8) & 0xffu;
+        bm <<= 8;
+        unsigned nb = 0;
 #pragma unroll
-        for (int f = 0; f < 4; f++) bm |= (ws.cav_nbr[4 * c + f] < 0 ? 1u : 0u) << f;
+        for (int f = 0; f < 4; f++) {
+            const int nc = ws.cav_nbr[4 * c + f];
+            bm |= (nc < 0 ? 1u : 0u) << f;
+            nb |= ((unsigned)nc & 0xffu) << (8 * f);
+        }
         RowEntry e;
-        e.fp = make_int4(fp[0], fp[1], fp[2], fp[3]);
-        e.tet = ws.cav_tet[c];
+        e.fp = make_int4(0, 0, 0, 0);
+        e.tet = tt;
         e.bmask = bm;
-        e.pad[0] = e.pad[1] = 0;
-        ent[o] = e;
+        e.nbr = (int)nb;
+        e.pos = 0;
+        ent[c] = e;
     }
     g.sync();
     return REC_DONE;
@@ -1320,9 +1336,14 @@ __device__ RowInfo volume_row(const MeshView &M, const dv3 q, W &ws, const Grp<G
         coincident_row<G>(M, q, ws, g, head.start, r);
         return r;
     }
-    for (int o = g.lane; o < ncav; o += G) {
-        ws.cav_tet[o] = ent[o].tet;
-        ws.bmask[o] = (uint8_t)ent[o].bmask;
+    // the record is in the flood's order: place each tet at its position in
+    // natinterp3d's visiting order
+    for (int e = g.lane; e < ncav; e += G) {
+        const RowEntry x = ent[e];
+        const int o = min(max(x.pos, 0), ncav - 1);  // a permutation of 0..ncav-1
+        ws.cav_tet[o] = x.tet;
+        ws.bmask[o] = (uint8_t)(x.bmask & 0xfu);
+        ws.eidx[o] = (uint8_t)e;
     }
     g.sync();
     auto face = [&](int k, int &c) {
@@ -1331,7 +1352,7 @@ __device__ RowInfo volume_row(const MeshView &M, const dv3 q, W &ws, const Grp<G
     };
     auto tet_fp = [&](int o, int &c, int (&fp)[4]) {
         c = o;
-        const int4 f = ent[o].fp;
+        const int4 f = ent[ws.eidx[o]].fp;
         fp[0] = f.x;
         fp[1] = f.y;
         fp[2] = f.z;
