@@ -1247,12 +1247,29 @@ __global__ void __launch_bounds__(32 * ORD_WARPS) k_rows_order(int64_t nrows, co
             while (w.start[lo + 1] <= k) lo++;
             return lo;
         };
-        for (int k = lane; k < total; k += 32) {
-            const int j = row_of(k), e = k - w.start[j];
-            const RowEntry x = ents[(s0 + j) * REC_CAV + e];
-            w.nbr[j][e] = x.nbr;
-            w.tet[j][e] = x.tet;
-            w.mir[j][e] = (uint8_t)(x.bmask >> 8);
+        // (tet, bmask, nbr, pos) of each entry in one 16-byte load, ORD_LOADS
+        // loads in flight a lane
+        constexpr int ORD_LOADS = 6;
+        for (int k0 = lane; k0 < total; k0 += 32 * ORD_LOADS) {
+            int4 x[ORD_LOADS];
+            int jj[ORD_LOADS], ee[ORD_LOADS];
+#pragma unroll
+            for (int u = 0; u < ORD_LOADS; u++) {
+                const int k = k0 + 32 * u;
+                if (k < total) {
+                    jj[u] = row_of(k);
+                    ee[u] = k - w.start[jj[u]];
+                    x[u] = reinterpret_cast<const int4 *>(ents + (s0 + jj[u]) * REC_CAV + ee[u])[1];
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < ORD_LOADS; u++) {
+                if (k0 + 32 * u < total) {
+                    w.tet[jj[u]][ee[u]] = x[u].x;
+                    w.mir[jj[u]][ee[u]] = (uint8_t)((unsigned)x[u].y >> 8);
+                    w.nbr[jj[u]][ee[u]] = x[u].z;
+                }
+            }
         }
         __syncwarp();
         if (nc > 0) {

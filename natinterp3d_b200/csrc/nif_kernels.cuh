@@ -37,6 +37,7 @@
 // one lane at a time, in a per-group global scratch, and counted).
 #pragma once
 #include <limits.h>
+#include <stddef.h>
 #include <stdint.h>
 
 #include "nif_exact.h"
@@ -556,6 +557,10 @@ struct __align__(32) RowEntry {
     int nbr;         // cavity indices of neighbours 0..3, one signed byte each
     int pos;         // position in natinterp3d's visiting order
 };
+// k_rows_order reads (tet, bmask, nbr, pos) as the entry's second int4
+static_assert(sizeof(RowEntry) == 32 && offsetof(RowEntry, tet) == 16 &&
+                  offsetof(RowEntry, bmask) == 20 && offsetof(RowEntry, nbr) == 24,
+              "RowEntry layout");
 
 __device__ __forceinline__ unsigned mix_hash(int key) {
     return (unsigned)key * 2654435761u;
