@@ -842,7 +842,32 @@ __device__ int flood_replay(const MeshView &M, const dv3 q, W &ws, const Grp<G> 
     g.sync();
     int qhead = 0, qtail = 1, ncav = 0;
     bool overflow = false;
-    while (qhead < qtail) {
+    // With natinterp3d's signs the located tet's neighbours join its wave:
+    // the flood tests them next whenever the located tet is in the cavity, in
+    // this same queue order, so the cavity indices are those of a flood that
+    // starts with the located tet alone, and one wave of a single lane is
+    // saved.  (If the located tet is not in the cavity, their tests are
+    // dropped below.)  Filtered modes keep the plain start, so that their
+    // predicate counters count the same tests.
+    const bool ring = !filt;
+    if (ring) {
+        int ns = -1;
+        bool full = false;
+        if (g.lane < 4) {
+            const int nb = comp(M.tn[start], g.lane);
+            bool fresh = false;
+            if (nb >= 0) {
+                const int sl = hash_insert(ws.u.a.hkey, W::HS, nb, fresh, full);
+                if (fresh) ns = sl;
+            }
+        }
+        const unsigned pm = g.ballot(ns >= 0);
+        if (ns >= 0) ws.u.a.queue[qtail + __popc(pm & g.lt())] = (slot_t)ns;
+        qtail += __popc(pm);
+        if (g.any(full)) overflow = true;
+        g.sync();
+    }
+    while (!overflow && qhead < qtail) {
         const int n = min(G, qtail - qhead);
         int slot = -1, tt = -1;
         bool inc = false, unc = false;
@@ -879,6 +904,7 @@ __device__ int flood_replay(const MeshView &M, const dv3 q, W &ws, const Grp<G> 
             }
         }
         const unsigned cm = g.ballot(inc);
+        if (ring && qhead == 0 && !(cm & 1u)) break;  // the located tet is outside: empty cavity
         const int ci = ncav + __popc(cm & g.lt());
         if (g.lane < n) ws.u.a.hval[slot] = (cav_t)(inc ? ci : -1);
         if (inc && ci < W::CAV) {
@@ -1162,45 +1188,45 @@ __device__ RowInfo row_volumes(const MeshView &M, const dv3 q, W &ws, const Grp<
                 g.sync();
             }
         };
-        // cavity-tet terms (natural_insertionfree.c:642-676)
-        for (int o0 = 0; o0 < ncav; o0 += G) {
-            const int o = o0 + g.lane;
-            const int nt_round = min(G, ncav - o0);
-            if (o < ncav) {
+        // cavity-tet terms (natural_insertionfree.c:642-676): one lane per
+        // item (tet o = k / 4, vertex k % 4), so that a cavity of 18 tets
+        // takes 3 lane-steps of 32 items rather than 4 steps of 18 lanes
+        for (int k0 = 0; k0 < 4 * ncav; k0 += PER) {
+            const int n_round = min(PER, 4 * ncav - k0);
+#pragma unroll 1
+            for (int k = k0 + g.lane; k < k0 + n_round; k += G) {
+                const int o = k >> 2, vi = k & 3;
                 int c, fp[4];
                 tet_fp(o, c, fp);
                 const int tt = ws.cav_tet[c];
                 const int4 p = M.tv[tt];
-#pragma unroll 1
-                for (int vi = 0; vi < 4; vi++) {
-                    const int v = comp(p, vi);
-                    const int sl = v < M.n ? neighbour_slot(ws, v) : -1;
-                    double term = 0.0;
-                    if (sl >= 0) {
-                        // the other three vertices in ascending slot order
-                        const int o0v = (vi == 0) ? 1 : 0;
-                        const int o1v = (vi <= 1) ? 2 : 1;
-                        const int o2v = (vi <= 2) ? 3 : 2;
-                        const dv3 pk = vload(M, v);
-                        const dv3 pa = vload(M, comp(p, o0v));
-                        const dv3 pb = vload(M, comp(p, o1v));
-                        const dv3 pc = vload(M, comp(p, o2v));
-                        const dv3 ct = cload(&M.tcc[tt]);
-                        // fp[] indexed through selects, so that it stays in registers
-                        auto pick = [&](int i) {
-                            return i == 0 ? fp[0] : (i == 1 ? fp[1] : (i == 2 ? fp[2] : fp[3]));
-                        };
-                        const dv3 f1 = cload(&M.fcc[pick(o2v)]);
-                        const dv3 f2 = cload(&M.fcc[pick(o1v)]);
-                        const dv3 f3 = cload(&M.fcc[pick(o0v)]);
-                        term = subcell_volume(pk, pa, pb, pc, ct, f1, f2, f3);
-                    }
-                    bterm[4 * g.lane + vi] = term;
-                    bslot[4 * g.lane + vi] = (int16_t)sl;
+                const int v = comp(p, vi);
+                const int sl = v < M.n ? neighbour_slot(ws, v) : -1;
+                double term = 0.0;
+                if (sl >= 0) {
+                    // the other three vertices in ascending slot order
+                    const int o0v = (vi == 0) ? 1 : 0;
+                    const int o1v = (vi <= 1) ? 2 : 1;
+                    const int o2v = (vi <= 2) ? 3 : 2;
+                    const dv3 pk = vload(M, v);
+                    const dv3 pa = vload(M, comp(p, o0v));
+                    const dv3 pb = vload(M, comp(p, o1v));
+                    const dv3 pc = vload(M, comp(p, o2v));
+                    const dv3 ct = cload(&M.tcc[tt]);
+                    // fp[] indexed through selects, so that it stays in registers
+                    auto pick = [&](int i) {
+                        return i == 0 ? fp[0] : (i == 1 ? fp[1] : (i == 2 ? fp[2] : fp[3]));
+                    };
+                    const dv3 f1 = cload(&M.fcc[pick(o2v)]);
+                    const dv3 f2 = cload(&M.fcc[pick(o1v)]);
+                    const dv3 f3 = cload(&M.fcc[pick(o0v)]);
+                    term = subcell_volume(pk, pa, pb, pc, ct, f1, f2, f3);
                 }
+                bterm[k - k0] = term;
+                bslot[k - k0] = (int16_t)sl;
             }
             g.sync();
-            fold(4 * nt_round);
+            fold(n_round);
         }
         // virtual-tet terms, query + boundary face (:681-719)
         for (int b0 = 0; b0 < nbf; b0 += G) {
