@@ -236,7 +236,7 @@ def run_reference(args, rank, world):
         'ms_per_step': sec * 1e3, 'higher_is_better': True, 'scaling': 'weak',
         'vs_baseline': None, 'dtype': 'f64', 'data': 'synthetic: seeded uniform keys and queries, '
                                                      'N(0,1) float32 values',
-        'config': plain_config(args, 1),
+        'config': plain_config(args, world),
         'cpu_baseline': {'value': value, 'unit': 'queries/s', 'cores': nthreads,
                          'kind': 'reference',
                          'sample': '%d of the %d queries per step (get_weights with %d OpenMP '

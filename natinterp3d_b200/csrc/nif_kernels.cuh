@@ -525,6 +525,8 @@ struct VolWorkspace {
         double buf[4 * G_ * 10 / 8];  // the fold's item buffer (4 G terms + slots); sink staging
     } u;
     double acc[NBR_];
+    int4 ctv[CAV_];     // vertex record of the o-th visited cavity tet
+    int4 cfp[CAV_];     // fcc[] indices of its faces (natinterp3d's face cache)
     int cav_tet[CAV_];  // cavity tets in visiting order
     int nbr_vid[NBR_];
     int vh_key[VH_];
@@ -532,7 +534,6 @@ struct VolWorkspace {
     uint16_t bface[BF_];
     int16_t vh_slot[VH_];
     uint8_t bmask[CAV_];  // boundary faces of each cavity tet, one bit per face
-    uint8_t eidx[CAV_];   // record entry of the o-th visited cavity tet
 };
 
 // One row between k_rows_cavity, k_rows_order and k_rows_volume: a header
@@ -1073,9 +1074,10 @@ __device__ __forceinline__ void face_cc_choice(const MeshView &M, const W &ws, i
 //   tet_fp(o, c, fp) the o-th tet in visiting order (index c into
 //                    ws.cav_tet) and the fcc[] indices of its four faces as
 //                    natinterp3d's face cache returns them
-template <int G, class W, bool FULL, class FaceFn, class FpFn>
+//   tet_tv(c)        the vertex record of cavity tet c (M.tv[ws.cav_tet[c]])
+template <int G, class W, bool FULL, class FaceFn, class FpFn, class TvFn>
 __device__ RowInfo row_volumes(const MeshView &M, const dv3 q, W &ws, const Grp<G> &g, const int ncav,
-                               RowInfo r, FaceFn face, FpFn tet_fp) {
+                               RowInfo r, FaceFn face, FpFn tet_fp, TvFn tet_tv) {
     // ---- 3. boundary faces (cavity order, then face order) ------------------
     int nbf = 0;
     for (int k0 = 0; k0 < 4 * ncav; k0 += G) {
@@ -1104,7 +1106,7 @@ __device__ RowInfo row_volumes(const MeshView &M, const dv3 q, W &ws, const Grp<
     for (int k = g.lane; k < 3 * nbf; k += G) {
         const int b = k / 3, j = k - 3 * b;
         const int cf = ws.bface[b];
-        const int v = comp(M.tv[ws.cav_tet[cf >> 2]], face_vslot(cf & 3, j));
+        const int v = comp(tet_tv(cf >> 2), face_vslot(cf & 3, j));
         if (v < M.n) {
             const int s = hash_upsert(ws.vh_key, W::VH, v, vfull);
             if (s >= 0) atomicMin(&ws.vh_first[s], k);
@@ -1123,7 +1125,7 @@ __device__ RowInfo row_volumes(const MeshView &M, const dv3 q, W &ws, const Grp<
         if (k < 3 * nbf) {
             const int b = k / 3, j = k - 3 * b;
             const int cf = ws.bface[b];
-            v = comp(M.tv[ws.cav_tet[cf >> 2]], face_vslot(cf & 3, j));
+            v = comp(tet_tv(cf >> 2), face_vslot(cf & 3, j));
             if (v < M.n) {
                 s = hash_find(ws.vh_key, W::VH, v);
                 first = (s >= 0) && ws.vh_first[s] == k;
@@ -1199,7 +1201,7 @@ __device__ RowInfo row_volumes(const MeshView &M, const dv3 q, W &ws, const Grp<
                 int c, fp[4];
                 tet_fp(o, c, fp);
                 const int tt = ws.cav_tet[c];
-                const int4 p = M.tv[tt];
+                const int4 p = tet_tv(c);
                 const int v = comp(p, vi);
                 const int sl = v < M.n ? neighbour_slot(ws, v) : -1;
                 double term = 0.0;
@@ -1236,7 +1238,7 @@ __device__ RowInfo row_volumes(const MeshView &M, const dv3 q, W &ws, const Grp<
                 const int cf = ws.bface[b];
                 const int f = cf & 3;
                 const int tt = ws.cav_tet[cf >> 2];
-                const int4 p = M.tv[tt];
+                const int4 p = tet_tv(cf >> 2);
                 const int va = comp(p, face_vslot(f, 0));
                 const int vb = comp(p, face_vslot(f, 1));
                 const int vc = comp(p, face_vslot(f, 2));
@@ -1313,7 +1315,8 @@ __device__ RowInfo sibson_row(const MeshView &M, const dv3 q, W &ws, const Grp<G
         c = ws.order[o];
         face_cc_choice(M, ws, c, fp);
     };
-    return row_volumes<G, W, FULL>(M, q, ws, g, ncav, r, face, tet_fp);
+    auto tet_tv = [&](int c) { return M.tv[ws.cav_tet[c]]; };
+    return row_volumes<G, W, FULL>(M, q, ws, g, ncav, r, face, tet_fp, tet_tv);
 }
 
 // The split row, part 1: cavity and visiting order of q around its located
@@ -1374,7 +1377,8 @@ __device__ RowInfo volume_row(const MeshView &M, const dv3 q, W &ws, const Grp<G
         const int o = min(max(x.pos, 0), ncav - 1);  // a permutation of 0..ncav-1
         ws.cav_tet[o] = x.tet;
         ws.bmask[o] = (uint8_t)(x.bmask & 0xfu);
-        ws.eidx[o] = (uint8_t)e;
+        ws.cfp[o] = x.fp;
+        ws.ctv[o] = M.tv[x.tet];
     }
     g.sync();
     auto face = [&](int k, int &c) {
@@ -1383,13 +1387,14 @@ __device__ RowInfo volume_row(const MeshView &M, const dv3 q, W &ws, const Grp<G
     };
     auto tet_fp = [&](int o, int &c, int (&fp)[4]) {
         c = o;
-        const int4 f = ent[ws.eidx[o]].fp;
+        const int4 f = ws.cfp[o];
         fp[0] = f.x;
         fp[1] = f.y;
         fp[2] = f.z;
         fp[3] = f.w;
     };
-    return row_volumes<G, W, FULL>(M, q, ws, g, ncav, r, face, tet_fp);
+    auto tet_tv = [&](int c) { return ws.ctv[c]; };
+    return row_volumes<G, W, FULL>(M, q, ws, g, ncav, r, face, tet_fp, tet_tv);
 }
 
 }  // namespace nif
