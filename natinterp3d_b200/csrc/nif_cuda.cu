@@ -1188,24 +1188,20 @@ __global__ void __launch_bounds__(FAST_BLOCK, OCC)
     }
 }
 
-// The split rows' visiting order: each record gets natinterp3d's LIFO
-// visiting order (natural_insertionfree.c:486-551, replayed on the cavity;
-// its non-cavity tets are leaves and do not change the order) and the fcc[]
-// indices of its faces as natinterp3d's face cache returns them (a face
-// shared with a cavity tet visited earlier reads that tet's copy through the
-// mirror slot, natural_insertionfree.c:233-253).  One warp takes 32
-// consecutive rows: the lanes load the rows' neighbour tables into shared
-// memory entry by entry, each lane replays one row there, and the lanes
-// write the positions and face choices back entry by entry.  Rows without a
-// cavity record are left alone.
+// The split rows' visiting order: each record entry gets its position in
+// natinterp3d's LIFO visiting order (natural_insertionfree.c:486-551,
+// replayed on the cavity; its non-cavity tets are leaves and do not change
+// the order).  k_rows_volume derives the face-cache choices from these
+// positions.  One warp takes 32 consecutive rows: the lanes load the rows'
+// neighbour bytes into shared memory entry by entry, each lane replays one
+// row there, and the lanes write the positions back entry by entry.  Rows
+// without a cavity record are left alone.
 constexpr int ORD_WARPS = 2;
 constexpr int ORD_PAD = REC_CAV + 1;  // row stride of the shared tables (banks)
 struct OrderWS {
     int nbr[32][ORD_PAD];
-    int tet[32][ORD_PAD];
     int8_t stack[32][4 * REC_CAV + 1];
     int8_t pos[32][REC_CAV];
-    uint8_t mir[32][REC_CAV];
     int start[33];
 };
 
@@ -1247,11 +1243,10 @@ __global__ void __launch_bounds__(32 * ORD_WARPS) k_rows_order(int64_t nrows, co
             while (w.start[lo + 1] <= k) lo++;
             return lo;
         };
-        // (tet, bmask, nbr, pos) of each entry in one 16-byte load, ORD_LOADS
-        // loads in flight a lane
+        // the neighbour bytes of each entry, ORD_LOADS loads in flight a lane
         constexpr int ORD_LOADS = 6;
         for (int k0 = lane; k0 < total; k0 += 32 * ORD_LOADS) {
-            int4 x[ORD_LOADS];
+            int x[ORD_LOADS];
             int jj[ORD_LOADS], ee[ORD_LOADS];
 #pragma unroll
             for (int u = 0; u < ORD_LOADS; u++) {
@@ -1259,16 +1254,12 @@ __global__ void __launch_bounds__(32 * ORD_WARPS) k_rows_order(int64_t nrows, co
                 if (k < total) {
                     jj[u] = row_of(k);
                     ee[u] = k - w.start[jj[u]];
-                    x[u] = reinterpret_cast<const int4 *>(ents + (s0 + jj[u]) * REC_CAV + ee[u])[1];
+                    x[u] = ents[(s0 + jj[u]) * REC_CAV + ee[u]].nbr;
                 }
             }
 #pragma unroll
             for (int u = 0; u < ORD_LOADS; u++) {
-                if (k0 + 32 * u < total) {
-                    w.tet[jj[u]][ee[u]] = x[u].x;
-                    w.mir[jj[u]][ee[u]] = (uint8_t)((unsigned)x[u].y >> 8);
-                    w.nbr[jj[u]][ee[u]] = x[u].z;
-                }
+                if (k0 + 32 * u < total) w.nbr[jj[u]][ee[u]] = x[u];
             }
         }
         __syncwarp();
@@ -1296,25 +1287,7 @@ __global__ void __launch_bounds__(32 * ORD_WARPS) k_rows_order(int64_t nrows, co
         __syncwarp();
         for (int k = lane; k < total; k += 32) {
             const int j = row_of(k), e = k - w.start[j];
-            const unsigned wd = (unsigned)w.nbr[j][e];
-            const int tt = w.tet[j][e];
-            const unsigned mir = w.mir[j][e];
-            const int pe = w.pos[j][e];
-            int fp[4];
-#pragma unroll
-            for (int i = 0; i < 4; i++) {
-                const int jf = 3 - i;
-                const int n = (int8_t)((wd >> (8 * jf)) & 0xffu);
-                if (n >= 0 && w.pos[j][n] < pe) {
-                    const int jm = (mir >> (2 * jf)) & 3;
-                    fp[i] = 4 * w.tet[j][n] + (3 - jm);
-                } else {
-                    fp[i] = 4 * tt + i;
-                }
-            }
-            RowEntry *E = ents + (s0 + j) * REC_CAV + e;
-            E->fp = make_int4(fp[0], fp[1], fp[2], fp[3]);
-            E->pos = pe;
+            ents[(s0 + j) * REC_CAV + e].pos = w.pos[j][e];
         }
         __syncwarp();
     }

@@ -528,6 +528,8 @@ struct VolWorkspace {
     int4 ctv[CAV_];     // vertex record of the o-th visited cavity tet
     int4 cfp[CAV_];     // fcc[] indices of its faces (natinterp3d's face cache)
     int cav_tet[CAV_];  // cavity tets in visiting order
+    int ftet[CAV_];     // cavity tets in the flood's order (the record's)
+    int8_t fpos[CAV_];  // visiting position of the e-th record entry
     int nbr_vid[NBR_];
     int vh_key[VH_];
     int vh_first[VH_];
@@ -541,8 +543,8 @@ struct VolWorkspace {
 // the cavity (bits 0-3) and the mirror slots of its faces (bits 8-15, the
 // mesh's tinfo bits 8-15), the cavity indices of its four neighbours (four
 // signed bytes, -1 outside the cavity); k_rows_order adds the tet's position
-// in natinterp3d's visiting order and the fcc[] indices of its faces'
-// circumcentres as natinterp3d's face cache returns them.
+// in natinterp3d's visiting order, from which k_rows_volume derives the fcc[]
+// indices of its faces' circumcentres as natinterp3d's face cache returns them.
 constexpr int REC_CAV = 48;  // cavity tets a record holds (larger cavities take the large kernel)
 constexpr int RS_OK = 0, RS_OUTSIDE = 1, RS_WALK = 2, RS_QUEUED = 3;
 struct __align__(16) RowHead {
@@ -551,17 +553,13 @@ struct __align__(16) RowHead {
     int state;  // RS_*
     int pad;
 };
-struct __align__(32) RowEntry {
-    int4 fp;
+struct __align__(16) RowEntry {
     int tet;
     unsigned bmask;  // boundary faces | mirror slots << 8
     int nbr;         // cavity indices of neighbours 0..3, one signed byte each
     int pos;         // position in natinterp3d's visiting order
 };
-// k_rows_order reads (tet, bmask, nbr, pos) as the entry's second int4
-static_assert(sizeof(RowEntry) == 32 && offsetof(RowEntry, tet) == 16 &&
-                  offsetof(RowEntry, bmask) == 20 && offsetof(RowEntry, nbr) == 24,
-              "RowEntry layout");
+static_assert(sizeof(RowEntry) == 16, "RowEntry is one 16-byte load");
 
 __device__ __forceinline__ unsigned mix_hash(int key) {
     return (unsigned)key * 2654435761u;
@@ -1348,7 +1346,6 @@ __device__ int cavity_record(const MeshView &M, const dv3 q, W &ws, const Grp<G>
             nb |= ((unsigned)nc & 0xffu) << (8 * f);
         }
         RowEntry e;
-        e.fp = make_int4(0, 0, 0, 0);
         e.tet = tt;
         e.bmask = bm;
         e.nbr = (int)nb;
@@ -1377,8 +1374,33 @@ __device__ RowInfo volume_row(const MeshView &M, const dv3 q, W &ws, const Grp<G
         const int o = min(max(x.pos, 0), ncav - 1);  // a permutation of 0..ncav-1
         ws.cav_tet[o] = x.tet;
         ws.bmask[o] = (uint8_t)(x.bmask & 0xfu);
-        ws.cfp[o] = x.fp;
         ws.ctv[o] = M.tv[x.tet];
+        ws.ftet[e] = x.tet;
+        ws.fpos[e] = (int8_t)o;
+    }
+    g.sync();
+    // natinterp3d's face cache (natural_insertionfree.c:233-253): a face
+    // shared with a cavity tet visited earlier returns that tet's copy, the
+    // mirror slot of the face in it; otherwise the tet's own slot
+    for (int e = g.lane; e < ncav; e += G) {
+        const RowEntry x = ent[e];
+        const int o = ws.fpos[e];
+        const int tt = ws.ftet[e];
+        const unsigned wd = (unsigned)x.nbr;
+        const unsigned mir = (x.bmask >> 8) & 0xffu;
+        int fp[4];
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            const int jf = 3 - i;
+            const int n = (int8_t)((wd >> (8 * jf)) & 0xffu);
+            if (n >= 0 && n < ncav && ws.fpos[n] < o) {
+                const int jm = (mir >> (2 * jf)) & 3;
+                fp[i] = 4 * ws.ftet[n] + (3 - jm);
+            } else {
+                fp[i] = 4 * tt + i;
+            }
+        }
+        ws.cfp[o] = make_int4(fp[0], fp[1], fp[2], fp[3]);
     }
     g.sync();
     auto face = [&](int k, int &c) {
