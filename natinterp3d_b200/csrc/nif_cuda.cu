@@ -1191,8 +1191,8 @@ __global__ void __launch_bounds__(FAST_BLOCK, OCC)
 // The split rows' visiting order: each record entry gets its position in
 // natinterp3d's LIFO visiting order (natural_insertionfree.c:486-551,
 // replayed on the cavity; its non-cavity tets are leaves and do not change
-// the order).  k_rows_volume derives the face-cache choices from these
-// positions.  One warp takes 32 consecutive rows: the lanes load the rows'
+// the order) and which of its faces take a neighbour's face-cache copy;
+// k_rows_volume derives the fcc[] indices from these.  One warp takes 32 consecutive rows: the lanes load the rows'
 // neighbour bytes into shared memory entry by entry, each lane replays one
 // row there, and the lanes write the positions back entry by entry.  Rows
 // without a cavity record are left alone.
@@ -1285,9 +1285,20 @@ __global__ void __launch_bounds__(32 * ORD_WARPS) k_rows_order(int64_t nrows, co
             }
         }
         __syncwarp();
+        // each entry's position, and in bits 8-11 which of its faces natinterp3d's
+        // face cache answers with a neighbour's copy (the neighbour across face
+        // 3 - i was visited earlier: bit i)
         for (int k = lane; k < total; k += 32) {
             const int j = row_of(k), e = k - w.start[j];
-            ents[(s0 + j) * REC_CAV + e].pos = w.pos[j][e];
+            const int pe = w.pos[j][e];
+            const unsigned wd = (unsigned)w.nbr[j][e];
+            unsigned take = 0;
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+                const int n = (int8_t)((wd >> (8 * (3 - i))) & 0xffu);
+                if (n >= 0 && w.pos[j][n] < pe) take |= 1u << i;
+            }
+            ents[(s0 + j) * REC_CAV + e].pos = pe | (int)(take << 8);
         }
         __syncwarp();
     }

@@ -557,7 +557,8 @@ struct __align__(16) RowEntry {
     int tet;
     unsigned bmask;  // boundary faces | mirror slots << 8
     int nbr;         // cavity indices of neighbours 0..3, one signed byte each
-    int pos;         // position in natinterp3d's visiting order
+    int pos;         // position in natinterp3d's visiting order (bits 0-7); bit 8 + i: face
+                     // 3 - i takes the copy of the neighbour visited earlier
 };
 static_assert(sizeof(RowEntry) == 16, "RowEntry is one 16-byte load");
 
@@ -1371,7 +1372,7 @@ __device__ RowInfo volume_row(const MeshView &M, const dv3 q, W &ws, const Grp<G
     // natinterp3d's visiting order
     for (int e = g.lane; e < ncav; e += G) {
         const RowEntry x = ent[e];
-        const int o = min(max(x.pos, 0), ncav - 1);  // a permutation of 0..ncav-1
+        const int o = min(x.pos & 0xff, ncav - 1);  // a permutation of 0..ncav-1
         ws.cav_tet[o] = x.tet;
         ws.bmask[o] = (uint8_t)(x.bmask & 0xfu);
         ws.ctv[o] = M.tv[x.tet];
@@ -1382,27 +1383,28 @@ __device__ RowInfo volume_row(const MeshView &M, const dv3 q, W &ws, const Grp<G
     // natinterp3d's face cache (natural_insertionfree.c:233-253): a face
     // shared with a cavity tet visited earlier returns that tet's copy, the
     // mirror slot of the face in it; otherwise the tet's own slot
+    // (k_rows_order marked those faces; cfp is first read after the syncs of
+    // the boundary-face step)
     for (int e = g.lane; e < ncav; e += G) {
         const RowEntry x = ent[e];
         const int o = ws.fpos[e];
-        const int tt = ws.ftet[e];
         const unsigned wd = (unsigned)x.nbr;
         const unsigned mir = (x.bmask >> 8) & 0xffu;
+        const unsigned take = ((unsigned)x.pos >> 8) & 0xfu;
         int fp[4];
 #pragma unroll
         for (int i = 0; i < 4; i++) {
             const int jf = 3 - i;
             const int n = (int8_t)((wd >> (8 * jf)) & 0xffu);
-            if (n >= 0 && n < ncav && ws.fpos[n] < o) {
+            if (((take >> i) & 1u) && n >= 0 && n < ncav) {
                 const int jm = (mir >> (2 * jf)) & 3;
                 fp[i] = 4 * ws.ftet[n] + (3 - jm);
             } else {
-                fp[i] = 4 * tt + i;
+                fp[i] = 4 * x.tet + i;
             }
         }
         ws.cfp[o] = make_int4(fp[0], fp[1], fp[2], fp[3]);
     }
-    g.sync();
     auto face = [&](int k, int &c) {
         c = k >> 2;
         return ((ws.bmask[c] >> (k & 3)) & 1u) != 0u;
