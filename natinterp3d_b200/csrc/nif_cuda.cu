@@ -1192,10 +1192,11 @@ __global__ void __launch_bounds__(FAST_BLOCK, OCC)
 // natinterp3d's LIFO visiting order (natural_insertionfree.c:486-551,
 // replayed on the cavity; its non-cavity tets are leaves and do not change
 // the order) and which of its faces take a neighbour's face-cache copy;
-// k_rows_volume derives the fcc[] indices from these.  One warp takes 32 consecutive rows: the lanes load the rows'
-// neighbour bytes into shared memory entry by entry, each lane replays one
-// row there, and the lanes write the positions back entry by entry.  Rows
-// without a cavity record are left alone.
+// k_rows_volume derives the fcc[] indices from these.  One warp takes 32
+// consecutive rows: the lanes load the rows' neighbour bytes into shared
+// memory entry by entry, each lane replays one row there, and the lanes
+// write the positions back entry by entry.  Rows without a cavity record
+// are left alone.
 constexpr int ORD_WARPS = 2;
 constexpr int ORD_PAD = REC_CAV + 1;  // row stride of the shared tables (banks)
 struct OrderWS {
