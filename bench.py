@@ -39,7 +39,7 @@ WORKLOAD = ('plain interpolate at scale: {keys:,} keys U[0,1]^3 float64, {querie
 
 # DRAM bytes (read + write) per row of one launch, from the ncu captures in
 # profiles/ (TRAFFIC_SOURCE)
-TRAFFIC_PER_ROW = {'k_rows_volume': (1.14e9 + 68.19e6) / 1_000_000}
+TRAFFIC_PER_ROW = {'k_rows_volume': (796.55e6 + 52.46e6) / 1_000_000}
 TRAFFIC_SOURCE = ('one 1,000,000-row k_rows_volume launch of the 1M-key / 10M-query workload '
                   '(dram__bytes_read.sum + dram__bytes_write.sum, 1 pass; '
                   'profiles/k_rows_volume_200k_keys_2M_queries.md)')
