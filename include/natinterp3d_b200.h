@@ -325,7 +325,7 @@ int nif_query_grad(const nif_dmesh *m, const void *d_queries, int query_dtype, i
 /* The same gradient without recomputing point location and cavities: the
  * forward keeps every row's cavity record (its cavity tets in natinterp3d's
  * visiting order, their face-circumcentre choices and boundary faces;
- * 784 bytes a row, nif_records_bytes) by calling
+ * 788 bytes a row, nif_records_bytes) by calling
  * nif_weights_count_records in place of nif_weights_count, then
  * nif_weights_fill as usual; nif_query_grad_records then takes that
  * workspace (unchanged since) and the records, for the same queries, M and

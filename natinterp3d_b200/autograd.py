@@ -8,7 +8,7 @@ and back-propagates into both arguments:
 * d/dqueries from the analytic derivative of the Sibson coordinates with
   respect to the query position (the GPU kernel differentiates the
   virtual-tet volumes, the only terms that move with the query).  The
-  forward keeps every row's cavity record (784 bytes a row) so that the
+  forward keeps every row's cavity record (788 bytes a row) so that the
   backward starts from it; beyond RECORDS_MAX_BYTES of records, or on meshes
   with other than the default fast predicates, the backward locates and
   floods each query's cavity again (same results, bit for bit).

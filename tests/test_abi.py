@@ -46,6 +46,19 @@ def test_cuda_size_queries_without_gpu():
     assert lib.nif_query_workspace_bytes(None, 10, 0, ctypes.byref(nb)) == _native.NIF_ERR_ARG
 
 
+def test_records_size_matches_the_header():
+    # the header documents 788 bytes a row of kept cavity records: a 16-byte
+    # head, 48 entries of 16 bytes and a 4-byte slot of the wide-row queue
+    from natinterp3d_b200 import _native
+    lib = _native.cuda_lib()
+    nb = ctypes.c_size_t()
+    M = 1_000_000
+    assert lib.nif_records_bytes(M, ctypes.byref(nb)) == 0
+    assert 788 * M <= nb.value <= 788 * M + 4096
+    assert lib.nif_records_bytes(0, ctypes.byref(nb)) == 0 and nb.value <= 4096
+    assert lib.nif_records_bytes(-1, ctypes.byref(nb)) == _native.NIF_ERR_ARG
+
+
 def test_mesh_export_is_consistent():
     from natinterp3d_b200._native import HostMesh
     rng = np.random.default_rng(0)
